@@ -1,0 +1,183 @@
+/*
+ * tdgl_b200.h — C ABI of the B200 trapezoidal TDGL stepper.
+ *
+ * Plain C: pointers, sizes and a CUDA stream handle.  Every entry point
+ * returns a tdgl_status; device pointers are owned by the caller and must
+ * stay valid until the stream has passed the call.  One context is used from
+ * one thread at a time; distinct contexts are independent.
+ *
+ * Layouts
+ *   reference layout  complex128 state of tdgl3d: blocks [psi, phi_x, phi_y,
+ *                     (phi_z)] of n_interior entries each, interior nodes in
+ *                     the order of GridIndices.interior_to_full (k fastest)
+ *                     (src/tdgl3d/core/state.py:11-97,
+ *                      src/tdgl3d/mesh/indices.py:271-278).  Stored as
+ *                     interleaved doubles (re, im); imaginary parts of phi
+ *                     are ignored on input and written as +0.0.
+ *   device layout     tdgl_state_len() doubles: component arrays psi_re,
+ *                     psi_im, phi_x, phi_y, (phi_z), each of tdgl_npad()
+ *                     entries, nodes numbered i fastest.  Padding entries
+ *                     must be zero.
+ *
+ * Each compute entry point names the reference function it replaces.
+ */
+#ifndef TDGL_B200_H
+#define TDGL_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* tdgl_stream_t; /* same handle as cudaStream_t */
+typedef struct tdgl_ctx tdgl_ctx;
+
+typedef enum tdgl_status {
+  TDGL_OK = 0,
+  TDGL_ENOCONV = 1,     /* Newton / TGCR did not converge (reference: empty array, converged=False, RuntimeError) */
+  TDGL_EDTMIN = 2,      /* adaptive dt fell below dt_min (integrators.py:190-195) */
+  TDGL_EKMAX = 3,       /* more Krylov directions needed than the workspace holds */
+  TDGL_ENONFINITE = 4,  /* a norm became NaN or Inf */
+  TDGL_ETIMEOUT = 5,    /* a device-side wait hit its time limit; the kernel returned */
+  TDGL_EINVAL = 6,      /* invalid argument (reference: ValueError) */
+  TDGL_ECUDA = 7,       /* CUDA runtime error */
+  TDGL_ENOMEM = 8       /* workspace allocation failed */
+} tdgl_status;
+
+typedef enum tdgl_precision {
+  TDGL_FP64 = 0,        /* Krylov vectors and Jacobian products in FP64 */
+  TDGL_MIXED = 1        /* Krylov vectors and analytic Jacobian products in FP32; state,
+                           residuals, norms and dot products in FP64 */
+} tdgl_precision;
+
+typedef enum tdgl_jvp_mode {
+  TDGL_JVP_FD = 0,       /* (f(x + eps p) - f(x)) / eps, eps = eps_mf (1 + |x|) / |p| (tgcr.py:129-133); FP64 only */
+  TDGL_JVP_ANALYTIC = 1  /* exact tangent-linear RHS */
+} tdgl_jvp_mode;
+
+/* Grid and physics (SimulationParameters, src/tdgl3d/core/parameters.py:10-51). */
+typedef struct tdgl_grid_desc {
+  int32_t Nx, Ny, Nz;                       /* cells; Nz == 1 is the 2-D model */
+  int32_t periodic_x, periodic_y, periodic_z;
+  double hx, hy, hz;
+  double kappa;                             /* used when kappa_full is NULL */
+} tdgl_grid_desc;
+
+/* Holes and materials, all host pointers, any may be NULL / zero-length.
+ * hole_*_links: GridIndices.hole_*_bc_mask (full-grid link indices);
+ * hole_*_interior: GridIndices.hole_*_bc_interior (reference interior numbering)
+ * (src/tdgl3d/mesh/indices.py:136-232).  kappa_full: MaterialMap.kappa (dim_x);
+ * sc_interior: MaterialMap.interior_sc_mask (n_interior); a NULL sc_interior
+ * means "no material map" (bare Ginzburg-Landau term, sparse_operators.py:218-226). */
+typedef struct tdgl_material_desc {
+  const int64_t* hole_links[3];
+  int64_t n_hole_links[3];
+  const int64_t* hole_interior[3];
+  int64_t n_hole_interior[3];
+  const double* kappa_full;
+  const double* sc_interior;
+} tdgl_material_desc;
+
+/* Applied field schedule (AppliedField, src/tdgl3d/physics/applied_field.py:14-56). */
+typedef struct tdgl_field {
+  double Bx, By, Bz;
+  double t_on_fraction, ramp_fraction;
+  double t_field_stop;                      /* the t_stop the schedule is relative to */
+  int32_t ramp;
+  int32_t constant;                         /* 1: (Bx,By,Bz) at every t, schedule ignored */
+} tdgl_field;
+
+/* Trapezoidal options (trapezoidal(), src/tdgl3d/solvers/integrators.py:92-118). */
+typedef struct tdgl_trap_opts {
+  double t_stop, dt, dt_min;
+  double newton_tol_f, newton_tol_dx, tol_gcr, eps_mf;
+  int32_t newton_max_iter;
+  int32_t krylov_max_iter;                  /* <= 0: the reference default, len(b) (capped by the workspace) */
+  int32_t adaptive;
+  int32_t jvp_mode;                         /* tdgl_jvp_mode */
+} tdgl_trap_opts;
+
+/* Counters and last values of one call. */
+typedef struct tdgl_stats {
+  int32_t status;
+  int32_t steps;                            /* accepted steps in this call */
+  int32_t newton_converged, newton_iters_last, krylov_last, max_krylov;
+  int64_t newton_iters, krylov_iters, rhs_evals, jvp_evals, rejections;
+  double t, dt_cur;                         /* integrator clock after the call */
+  double last_gnorm, last_dxnorm;
+  int64_t kernel_launches;
+} tdgl_stats;
+
+/* ---- context ------------------------------------------------------------ */
+
+/* Build the device description of a grid (construct_indices + material map,
+ * src/tdgl3d/mesh/indices.py:239-450, src/tdgl3d/core/material.py:182-254).
+ * precision: tdgl_precision.  kmax: Krylov directions the workspace holds (>= 1). */
+int tdgl_ctx_create(const tdgl_grid_desc* grid, const tdgl_material_desc* material, int32_t precision,
+                    int32_t kmax, tdgl_ctx** out);
+int tdgl_ctx_destroy(tdgl_ctx* ctx);
+int64_t tdgl_n_interior(const tdgl_ctx* ctx);
+int64_t tdgl_npad(const tdgl_ctx* ctx);
+int64_t tdgl_state_len(const tdgl_ctx* ctx);        /* doubles of one device-layout state */
+int64_t tdgl_workspace_bytes(const tdgl_ctx* ctx);  /* device bytes the context holds */
+const char* tdgl_status_string(int status);
+const char* tdgl_last_error(void);                  /* text of the last failure on this thread */
+
+/* ---- layout -------------------------------------------------------------- */
+
+/* Reference layout (2*n_state doubles) -> device layout. */
+int tdgl_pack(tdgl_ctx* ctx, const double* x_ref, double* x_dev, tdgl_stream_t stream);
+/* Device layout -> reference layout. */
+int tdgl_unpack(tdgl_ctx* ctx, const double* x_dev, double* x_ref, tdgl_stream_t stream);
+
+/* ---- operators ----------------------------------------------------------- */
+
+/* f = dX/dt in the device layout.  Replaces eval_f (src/tdgl3d/physics/rhs.py:147-239)
+ * with the applied field (Bx, By, Bz) placed as build_boundary_field_vectors does. */
+int tdgl_rhs(tdgl_ctx* ctx, const double* x_dev, double* f_dev, double Bx, double By, double Bz,
+             tdgl_stream_t stream);
+/* eval_f on reference-layout device buffers (pack, RHS, unpack). */
+int tdgl_eval_f(tdgl_ctx* ctx, const double* x_ref, double* f_ref, double Bx, double By, double Bz,
+                tdgl_stream_t stream);
+/* ap = p - dt/2 J(x) p in the device layout (the A*p of tgcr_matrix_free_trap,
+ * src/tdgl3d/solvers/tgcr.py:129-133).  mode FD uses eps = eps_mf (1+|x|)/|p|. */
+int tdgl_jvp(tdgl_ctx* ctx, const double* x_dev, const double* p_dev, double* ap_dev, double dt, int32_t mode,
+             double eps_mf, double Bx, double By, double Bz, tdgl_stream_t stream);
+/* Observables at interior nodes in reference order (n_interior doubles each):
+ * |psi|^2 (solution.py:76-78), B with boundary conditions (solution.py:94-158),
+ * J_s without boundary conditions (solution.py:180-217). */
+int tdgl_observables(tdgl_ctx* ctx, const double* x_dev, double Bx, double By, double Bz, double* psi2,
+                     double* bx, double* by, double* bz, double* jx, double* jy, double* jz,
+                     tdgl_stream_t stream);
+
+/* ---- solvers (device-resident control; blocking: returns after the stream work) ---- */
+
+/* Solve (I - dt/2 J(x_lin)) d = b.  Replaces tgcr_matrix_free_trap
+ * (src/tdgl3d/solvers/tgcr.py:96-156).  Returns TDGL_ENOCONV when the relative
+ * residual stays above tol (the reference returns an empty array). */
+int tdgl_tgcr_trap(tdgl_ctx* ctx, const double* x_lin_dev, const double* b_dev, double* d_dev, double dt,
+                   double tol, int32_t max_iter, double eps_mf, int32_t jvp_mode, double Bx, double By,
+                   double Bz, tdgl_stats* stats, tdgl_stream_t stream);
+/* Newton on x - dt/2 f(x) - gamma = 0 from x (updated in place).  Replaces
+ * newton_gcr_trap (src/tdgl3d/solvers/newton.py:76-120); convergence is
+ * reported in stats->newton_converged and iterations in stats->newton_iters_last. */
+int tdgl_newton_trap(tdgl_ctx* ctx, double* x_dev, const double* gamma_dev, double dt, double tol_f,
+                     double tol_dx, int32_t max_iter, double tol_gcr, double eps_mf, int32_t jvp_mode,
+                     double Bx, double By, double Bz, tdgl_stats* stats, tdgl_stream_t stream);
+/* Advance x (device layout, in place) through at most max_steps accepted
+ * trapezoidal steps from *t with step *dt_cur (both updated).  Replaces the
+ * loop of trapezoidal (src/tdgl3d/solvers/integrators.py:150-197). */
+int tdgl_trap_run(tdgl_ctx* ctx, double* x_dev, double* t, double* dt_cur, int32_t max_steps,
+                  const tdgl_trap_opts* opts, const tdgl_field* field, tdgl_stats* stats, tdgl_stream_t stream);
+/* Forward Euler: n_steps steps of min(dt, t_stop - t) from *t (updated)
+ * (src/tdgl3d/solvers/integrators.py:35-89). */
+int tdgl_euler_run(tdgl_ctx* ctx, double* x_dev, double* t, double t_stop, double dt, int32_t n_steps,
+                   const tdgl_field* field, tdgl_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TDGL_B200_H */

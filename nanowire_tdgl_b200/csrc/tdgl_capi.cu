@@ -1,0 +1,495 @@
+// C ABI of the B200 TDGL stepper (include/tdgl_b200.h): context set-up,
+// workspace, launches.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "tdgl_b200.h"
+#include "tdgl_geometry.h"
+#include "tdgl_stepper.cuh"
+
+using namespace tdgl;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+#define TDGL_CUDA(call)                                                                 \
+  do {                                                                                  \
+    cudaError_t e_ = (call);                                                            \
+    if (e_ != cudaSuccess)                                                              \
+      return fail(TDGL_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_));      \
+  } while (0)
+
+
+}  // namespace
+
+struct tdgl_ctx {
+  Grid g{};
+  int precision = TDGL_FP64;
+  int kmax = 0;
+  int device = 0;
+  int num_sms = 0;
+  long L = 0;           // doubles (or floats) of one device-layout vector
+  size_t bytes = 0;
+  // geometry
+  uint8_t* lflags = nullptr;
+  uint8_t* nflags = nullptr;
+  double* k2 = nullptr;
+  double* sc = nullptr;
+  // scratch for the reference-layout operators
+  double* s_x = nullptr;
+  double* s_f = nullptr;
+  double* s_red = nullptr;
+  // solver workspace (allocated on first use)
+  bool ws_ready = false;
+  double* X1 = nullptr;
+  double* G = nullptr;
+  double* F = nullptr;
+  void* R[3] = {nullptr, nullptr, nullptr};
+  void* XL = nullptr;
+  void* P = nullptr;
+  void* AP = nullptr;
+  double* partials = nullptr;
+  double* results = nullptr;
+  unsigned* bar = nullptr;
+  int* err = nullptr;
+  Ctl* ctl_dev = nullptr;
+  Ctl* ctl_host = nullptr;
+  int blocks = 0;
+  size_t smem = 0;
+  std::vector<void*> owned;
+};
+
+static int ctx_alloc(tdgl_ctx* c, void** p, size_t bytes) {
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) return fail(TDGL_ENOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  c->owned.push_back(*p);
+  c->bytes += bytes;
+  e = cudaMemset(*p, 0, bytes);
+  if (e != cudaSuccess) return fail(TDGL_ECUDA, std::string("cudaMemset: ") + cudaGetErrorString(e));
+  return TDGL_OK;
+}
+
+extern "C" const char* tdgl_status_string(int s) {
+  switch (s) {
+    case TDGL_OK: return "ok";
+    case TDGL_ENOCONV: return "did not converge";
+    case TDGL_EDTMIN: return "dt reduced below dt_min";
+    case TDGL_EKMAX: return "Krylov workspace exhausted";
+    case TDGL_ENONFINITE: return "non-finite value";
+    case TDGL_ETIMEOUT: return "device wait timed out";
+    case TDGL_EINVAL: return "invalid argument";
+    case TDGL_ECUDA: return "CUDA error";
+    case TDGL_ENOMEM: return "out of device memory";
+    default: return "unknown status";
+  }
+}
+
+extern "C" const char* tdgl_last_error(void) { return g_last_error.c_str(); }
+
+extern "C" int tdgl_ctx_create(const tdgl_grid_desc* gd, const tdgl_material_desc* md, int32_t precision,
+                               int32_t kmax, tdgl_ctx** out) {
+  if (!gd || !out) return fail(TDGL_EINVAL, "null argument");
+  *out = nullptr;
+  if (precision != TDGL_FP64 && precision != TDGL_MIXED) return fail(TDGL_EINVAL, "unknown precision");
+  if (kmax < 1) return fail(TDGL_EINVAL, "kmax must be >= 1");
+  HostGeometry hg;
+  std::string msg;
+  int rc = build_geometry(gd, md, hg, msg);
+  if (rc) return fail(rc, msg);
+  tdgl_ctx* c = new tdgl_ctx();
+  c->precision = precision;
+  c->kmax = kmax;
+  cudaGetDevice(&c->device);
+  cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device);
+  c->g = hg.g;
+  Grid& g = c->g;
+  c->L = (long)g.ncomp * g.npad;
+  const long n = g.n;
+  if ((rc = ctx_alloc(c, (void**)&c->nflags, n))) { tdgl_ctx_destroy(c); return rc; }
+  TDGL_CUDA(cudaMemcpy(c->nflags, hg.nflags.data(), n, cudaMemcpyHostToDevice));
+  g.nflags = c->nflags;
+  if (!hg.lflags.empty()) {
+    if ((rc = ctx_alloc(c, (void**)&c->lflags, hg.lflags.size()))) { tdgl_ctx_destroy(c); return rc; }
+    TDGL_CUDA(cudaMemcpy(c->lflags, hg.lflags.data(), hg.lflags.size(), cudaMemcpyHostToDevice));
+  }
+  g.lflags = c->lflags;
+  if (!hg.k2.empty()) {
+    if ((rc = ctx_alloc(c, (void**)&c->k2, n * sizeof(double)))) { tdgl_ctx_destroy(c); return rc; }
+    TDGL_CUDA(cudaMemcpy(c->k2, hg.k2.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  g.k2int = c->k2;
+  if (!hg.sc.empty()) {
+    if ((rc = ctx_alloc(c, (void**)&c->sc, n * sizeof(double)))) { tdgl_ctx_destroy(c); return rc; }
+    TDGL_CUDA(cudaMemcpy(c->sc, hg.sc.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  g.scint = c->sc;
+  const size_t vbytes = (size_t)c->L * sizeof(double);
+  if ((rc = ctx_alloc(c, (void**)&c->s_x, vbytes))) { tdgl_ctx_destroy(c); return rc; }
+  if ((rc = ctx_alloc(c, (void**)&c->s_f, vbytes))) { tdgl_ctx_destroy(c); return rc; }
+  if ((rc = ctx_alloc(c, (void**)&c->s_red, 64 * sizeof(double)))) { tdgl_ctx_destroy(c); return rc; }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) { tdgl_ctx_destroy(c); return fail(TDGL_ECUDA, cudaGetErrorString(e)); }
+  *out = c;
+  return TDGL_OK;
+}
+
+extern "C" int tdgl_ctx_destroy(tdgl_ctx* c) {
+  if (!c) return TDGL_OK;
+  for (void* p : c->owned) cudaFree(p);
+  if (c->ctl_host) cudaFreeHost(c->ctl_host);
+  delete c;
+  return TDGL_OK;
+}
+
+extern "C" int64_t tdgl_n_interior(const tdgl_ctx* c) { return c ? c->g.n : -1; }
+extern "C" int64_t tdgl_npad(const tdgl_ctx* c) { return c ? c->g.npad : -1; }
+extern "C" int64_t tdgl_state_len(const tdgl_ctx* c) { return c ? c->L : -1; }
+extern "C" int64_t tdgl_workspace_bytes(const tdgl_ctx* c) { return c ? (int64_t)c->bytes : -1; }
+
+static int grid_1d(const tdgl_ctx* c, long work) {
+  long b = (work + kThreads - 1) / kThreads;
+  long cap = (long)c->num_sms * 4;
+  return (int)std::max(1L, std::min(b, cap));
+}
+
+extern "C" int tdgl_pack(tdgl_ctx* c, const double* x_ref, double* x_dev, tdgl_stream_t s) {
+  if (!c || !x_ref || !x_dev) return fail(TDGL_EINVAL, "null argument");
+  k_pack<<<grid_1d(c, c->g.n), kThreads, 0, s>>>(c->g, (const double2*)x_ref, x_dev);
+  TDGL_CUDA(cudaGetLastError());
+  return TDGL_OK;
+}
+
+extern "C" int tdgl_unpack(tdgl_ctx* c, const double* x_dev, double* x_ref, tdgl_stream_t s) {
+  if (!c || !x_ref || !x_dev) return fail(TDGL_EINVAL, "null argument");
+  k_unpack<<<grid_1d(c, c->g.n), kThreads, 0, s>>>(c->g, x_dev, (double2*)x_ref);
+  TDGL_CUDA(cudaGetLastError());
+  return TDGL_OK;
+}
+
+extern "C" int tdgl_rhs(tdgl_ctx* c, const double* x, double* f, double Bx, double By, double Bz, tdgl_stream_t s) {
+  if (!c || !x || !f) return fail(TDGL_EINVAL, "null argument");
+  k_rhs<<<grid_1d(c, c->g.n), kThreads, 0, s>>>(c->g, x, f, bterms(c->g, Bx, By, Bz));
+  TDGL_CUDA(cudaGetLastError());
+  return TDGL_OK;
+}
+
+extern "C" int tdgl_eval_f(tdgl_ctx* c, const double* x_ref, double* f_ref, double Bx, double By, double Bz,
+                           tdgl_stream_t s) {
+  int rc;
+  if ((rc = tdgl_pack(c, x_ref, c->s_x, s))) return rc;
+  if ((rc = tdgl_rhs(c, c->s_x, c->s_f, Bx, By, Bz, s))) return rc;
+  return tdgl_unpack(c, c->s_f, f_ref, s);
+}
+
+// sum of squares of a device-layout FP64 vector (single block, deterministic)
+__global__ void k_norm2(const double* __restrict__ v, long L, double* out) {
+  double s = 0.0;
+  for (long e = threadIdx.x; e < L; e += blockDim.x) s += v[e] * v[e];
+  s = warp_sum(s);
+  __shared__ double w[kWarps];
+  if ((threadIdx.x & 31) == 0) w[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int i = 0; i < kWarps; ++i) t += w[i];
+    *out = t;
+  }
+}
+
+extern "C" int tdgl_jvp(tdgl_ctx* c, const double* x, const double* p, double* ap, double dt, int32_t mode,
+                        double eps_mf, double Bx, double By, double Bz, tdgl_stream_t s) {
+  if (!c || !x || !p || !ap) return fail(TDGL_EINVAL, "null argument");
+  BTerms<double> b = bterms(c->g, Bx, By, Bz);
+  if (mode == TDGL_JVP_ANALYTIC) {
+    k_jvp_analytic<double><<<grid_1d(c, c->g.n), kThreads, 0, s>>>(c->g, x, p, ap, dt / 2.0, b);
+    TDGL_CUDA(cudaGetLastError());
+    return TDGL_OK;
+  }
+  if (mode != TDGL_JVP_FD) return fail(TDGL_EINVAL, "unknown jvp mode");
+  k_rhs<<<grid_1d(c, c->g.n), kThreads, 0, s>>>(c->g, x, c->s_f, b);
+  k_norm2<<<1, kThreads, 0, s>>>(x, c->L, c->s_red);
+  k_norm2<<<1, kThreads, 0, s>>>(p, c->L, c->s_red + 1);
+  double h[2];
+  TDGL_CUDA(cudaMemcpyAsync(h, c->s_red, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+  TDGL_CUDA(cudaStreamSynchronize(s));
+  double pn = std::sqrt(h[1]);
+  if (pn == 0.0) return fail(TDGL_EINVAL, "zero direction");
+  double eps = eps_mf * (1.0 + std::sqrt(h[0])) / pn;
+  k_jvp_fd<<<grid_1d(c, c->g.n), kThreads, 0, s>>>(c->g, x, c->s_f, p, ap, dt / 2.0, eps, b);
+  TDGL_CUDA(cudaGetLastError());
+  return TDGL_OK;
+}
+
+extern "C" int tdgl_observables(tdgl_ctx* c, const double* x, double Bx, double By, double Bz, double* psi2,
+                                double* bx, double* by, double* bz, double* jx, double* jy, double* jz,
+                                tdgl_stream_t s) {
+  if (!c || !x || !psi2 || !bx || !by || !bz || !jx || !jy || !jz) return fail(TDGL_EINVAL, "null argument");
+  const Grid& g = c->g;
+  k_observables<<<grid_1d(c, g.n), kThreads, 0, s>>>(g, x, bterms(g, Bx, By, Bz), 1.0 / (g.hx * g.hy),
+                                                      1.0 / (g.hy * g.hz), 1.0 / (g.hz * g.hx), psi2, bx, by, bz,
+                                                      jx, jy, jz);
+  TDGL_CUDA(cudaGetLastError());
+  return TDGL_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Solver workspace and the persistent launch
+// ---------------------------------------------------------------------------
+
+template <typename T>
+static int setup_launch(tdgl_ctx* c) {
+  int nacc = c->kmax + 4;
+  c->smem = (size_t)(kWarps * nacc + 2 * nacc + 3 * c->kmax) * sizeof(double);
+  if (c->smem > 48 * 1024)
+    TDGL_CUDA(cudaFuncSetAttribute(k_stepper<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem));
+  int occ = 0;
+  TDGL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stepper<T>, kThreads, c->smem));
+  if (occ < 1) return fail(TDGL_ECUDA, "stepper kernel does not fit on an SM");
+  c->blocks = c->num_sms * std::min(occ, 1);
+  return TDGL_OK;
+}
+
+static int ensure_workspace(tdgl_ctx* c) {
+  if (c->ws_ready) return TDGL_OK;
+  const size_t vb = (size_t)c->L * sizeof(double);
+  const size_t tb = (size_t)c->L * (c->precision == TDGL_MIXED ? sizeof(float) : sizeof(double));
+  int rc;
+  if ((rc = ctx_alloc(c, (void**)&c->X1, vb))) return rc;
+  if ((rc = ctx_alloc(c, (void**)&c->G, vb))) return rc;
+  if ((rc = ctx_alloc(c, (void**)&c->F, vb))) return rc;
+  for (int i = 0; i < 3; ++i)
+    if ((rc = ctx_alloc(c, &c->R[i], tb))) return rc;
+  if (c->precision == TDGL_MIXED)
+    if ((rc = ctx_alloc(c, &c->XL, tb))) return rc;
+  if ((rc = ctx_alloc(c, &c->P, tb * c->kmax))) return rc;
+  if ((rc = ctx_alloc(c, &c->AP, tb * c->kmax))) return rc;
+  rc = c->precision == TDGL_MIXED ? setup_launch<float>(c) : setup_launch<double>(c);
+  if (rc) return rc;
+  int nslot = c->kmax + 4;
+  if ((rc = ctx_alloc(c, (void**)&c->partials, sizeof(double) * nslot * (size_t)c->blocks))) return rc;
+  if ((rc = ctx_alloc(c, (void**)&c->results, sizeof(double) * nslot))) return rc;
+  if ((rc = ctx_alloc(c, (void**)&c->bar, 4 * sizeof(unsigned)))) return rc;
+  if ((rc = ctx_alloc(c, (void**)&c->err, 4 * sizeof(int)))) return rc;
+  if ((rc = ctx_alloc(c, (void**)&c->ctl_dev, sizeof(Ctl)))) return rc;
+  TDGL_CUDA(cudaMallocHost((void**)&c->ctl_host, sizeof(Ctl)));
+  c->ws_ready = true;
+  return TDGL_OK;
+}
+
+template <typename T>
+static StepArgs<T> make_args(tdgl_ctx* c, double* x0, double* x1, double* G, double* D) {
+  StepArgs<T> A{};
+  A.g = c->g;
+  A.sy.partials = c->partials;
+  A.sy.results = c->results;
+  A.sy.bar = c->bar;
+  A.sy.err = c->err;
+  A.sy.nslot_max = c->kmax + 4;
+  A.sy.timeout_ns = 5000000000ull;
+  A.ctl = c->ctl_dev;
+  A.X[0] = x0;
+  A.X[1] = x1;
+  A.G = G;
+  A.F = c->F;
+  A.D = D;
+  for (int i = 0; i < 3; ++i) A.R[i] = (T*)c->R[i];
+  A.XL = (T*)c->XL;
+  A.P = (T*)c->P;
+  A.AP = (T*)c->AP;
+  A.kmax = c->kmax;
+  A.L = c->L;
+  return A;
+}
+
+// Launch the persistent kernel with the control block in c->ctl_host; on
+// return c->ctl_host holds the outputs.
+static int run_stepper(tdgl_ctx* c, double* x0, double* x1, double* G, double* D, tdgl_stream_t s) {
+  TDGL_CUDA(cudaMemsetAsync(c->bar, 0, 4 * sizeof(unsigned), s));
+  TDGL_CUDA(cudaMemsetAsync(c->err, 0, 4 * sizeof(int), s));
+  TDGL_CUDA(cudaMemcpyAsync(c->ctl_dev, c->ctl_host, sizeof(Ctl), cudaMemcpyHostToDevice, s));
+  if (c->precision == TDGL_MIXED) {
+    StepArgs<float> A = make_args<float>(c, x0, x1, G, D);
+    void* args[] = {&A};
+    TDGL_CUDA(cudaLaunchCooperativeKernel((void*)k_stepper<float>, c->blocks, kThreads, args, c->smem, s));
+  } else {
+    StepArgs<double> A = make_args<double>(c, x0, x1, G, D);
+    void* args[] = {&A};
+    TDGL_CUDA(cudaLaunchCooperativeKernel((void*)k_stepper<double>, c->blocks, kThreads, args, c->smem, s));
+  }
+  int herr = 0;
+  TDGL_CUDA(cudaMemcpyAsync(c->ctl_host, c->ctl_dev, sizeof(Ctl), cudaMemcpyDeviceToHost, s));
+  TDGL_CUDA(cudaMemcpyAsync(&herr, c->err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  TDGL_CUDA(cudaStreamSynchronize(s));
+  if (herr) c->ctl_host->status = herr;
+  return TDGL_OK;
+}
+
+static void fill_stats(const tdgl_ctx* c, tdgl_stats* st) {
+  if (!st) return;
+  const Ctl& k = *c->ctl_host;
+  st->status = k.status;
+  st->steps = k.steps;
+  st->newton_converged = k.newton_converged;
+  st->newton_iters_last = k.newton_iters_last;
+  st->krylov_last = k.krylov_last;
+  st->max_krylov = k.max_krylov;
+  st->newton_iters = k.newton_iters;
+  st->krylov_iters = k.krylov_iters;
+  st->rhs_evals = k.rhs_evals;
+  st->jvp_evals = k.jvp_evals;
+  st->rejections = k.rejections;
+  st->t = k.t;
+  st->dt_cur = k.dt_cur;
+  st->last_gnorm = k.last_gnorm;
+  st->last_dxnorm = k.last_dxnorm;
+  st->kernel_launches = 1;
+}
+
+static void ctl_reset(tdgl_ctx* c) {
+  std::memset(c->ctl_host, 0, sizeof(Ctl));
+  c->ctl_host->field_const = 1;
+}
+
+static int krylov_cap(const tdgl_ctx* c, int32_t max_iter) {
+  // the reference default is len(b) = n_state; the workspace bound is enforced on the device
+  long ref = (long)(c->g.ncomp - 1) * c->g.n;
+  return max_iter > 0 ? max_iter : (int)std::min(ref, (long)1 << 30);
+}
+
+template <typename T>
+__global__ void k_to_t(const double* __restrict__ a, T* __restrict__ b, long L) {
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < L; e += (long)gridDim.x * blockDim.x) b[e] = (T)a[e];
+}
+
+extern "C" int tdgl_tgcr_trap(tdgl_ctx* c, const double* x_lin, const double* bvec, double* dvec, double dt,
+                              double tol, int32_t max_iter, double eps_mf, int32_t jvp_mode, double Bx, double By,
+                              double Bz, tdgl_stats* st, tdgl_stream_t s) {
+  if (!c || !x_lin || !bvec || !dvec) return fail(TDGL_EINVAL, "null argument");
+  if (jvp_mode == TDGL_JVP_FD && c->precision == TDGL_MIXED)
+    return fail(TDGL_EINVAL, "the finite-difference product needs the FP64 context");
+  int rc;
+  if ((rc = ensure_workspace(c))) return rc;
+  if (c->precision == TDGL_MIXED) k_to_t<float><<<grid_1d(c, c->L), kThreads, 0, s>>>(bvec, (float*)c->R[0], c->L);
+  else TDGL_CUDA(cudaMemcpyAsync(c->R[0], bvec, c->L * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  ctl_reset(c);
+  Ctl& k = *c->ctl_host;
+  k.run_mode = RUN_TGCR;
+  k.dt = dt;
+  k.tol_gcr = tol;
+  k.krylov_max_iter = krylov_cap(c, max_iter);
+  k.eps_mf = eps_mf;
+  k.jvp_mode = jvp_mode;
+  k.Bx = Bx; k.By = By; k.Bz = Bz;
+  if ((rc = run_stepper(c, const_cast<double*>(x_lin), c->X1, c->G, dvec, s))) return rc;
+  fill_stats(c, st);
+  return c->ctl_host->status;
+}
+
+extern "C" int tdgl_newton_trap(tdgl_ctx* c, double* x, const double* gamma, double dt, double tol_f,
+                                double tol_dx, int32_t max_iter, double tol_gcr, double eps_mf, int32_t jvp_mode,
+                                double Bx, double By, double Bz, tdgl_stats* st, tdgl_stream_t s) {
+  if (!c || !x || !gamma) return fail(TDGL_EINVAL, "null argument");
+  if (jvp_mode == TDGL_JVP_FD && c->precision == TDGL_MIXED)
+    return fail(TDGL_EINVAL, "the finite-difference product needs the FP64 context");
+  int rc;
+  if ((rc = ensure_workspace(c))) return rc;
+  ctl_reset(c);
+  Ctl& k = *c->ctl_host;
+  k.run_mode = RUN_NEWTON;
+  k.dt = dt;
+  k.tol_f = tol_f;
+  k.tol_dx = tol_dx;
+  k.newton_max_iter = max_iter;
+  k.tol_gcr = tol_gcr;
+  k.krylov_max_iter = krylov_cap(c, 0);
+  k.eps_mf = eps_mf;
+  k.jvp_mode = jvp_mode;
+  k.Bx = Bx; k.By = By; k.Bz = Bz;
+  k.cur = 0;
+  if ((rc = run_stepper(c, x, c->X1, const_cast<double*>(gamma), nullptr, s))) return rc;
+  fill_stats(c, st);
+  return c->ctl_host->status;
+}
+
+extern "C" int tdgl_trap_run(tdgl_ctx* c, double* x, double* t, double* dt_cur, int32_t max_steps,
+                             const tdgl_trap_opts* o, const tdgl_field* f, tdgl_stats* st, tdgl_stream_t s) {
+  if (!c || !x || !t || !dt_cur || !o || !f) return fail(TDGL_EINVAL, "null argument");
+  if (o->jvp_mode == TDGL_JVP_FD && c->precision == TDGL_MIXED)
+    return fail(TDGL_EINVAL, "the finite-difference product needs the FP64 context");
+  int rc;
+  if ((rc = ensure_workspace(c))) return rc;
+  ctl_reset(c);
+  Ctl& k = *c->ctl_host;
+  k.run_mode = RUN_TRAP;
+  k.t_stop = o->t_stop;
+  k.dt = o->dt;
+  k.dt_min = o->dt_min;
+  k.tol_f = o->newton_tol_f;
+  k.tol_dx = o->newton_tol_dx;
+  k.tol_gcr = o->tol_gcr;
+  k.eps_mf = o->eps_mf;
+  k.newton_max_iter = o->newton_max_iter;
+  k.krylov_max_iter = krylov_cap(c, o->krylov_max_iter);
+  k.adaptive = o->adaptive;
+  k.jvp_mode = o->jvp_mode;
+  k.max_steps = max_steps;
+  k.Bx = f->Bx; k.By = f->By; k.Bz = f->Bz;
+  k.t_on_fraction = f->t_on_fraction;
+  k.ramp_fraction = f->ramp_fraction;
+  k.t_field_stop = f->t_field_stop;
+  k.ramp = f->ramp;
+  k.field_const = f->constant;
+  k.t = *t;
+  k.dt_cur = *dt_cur;
+  k.cur = 0;
+  if ((rc = run_stepper(c, x, c->X1, c->G, nullptr, s))) return rc;
+  if (c->ctl_host->cur == 1) {
+    TDGL_CUDA(cudaMemcpyAsync(x, c->X1, c->L * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    TDGL_CUDA(cudaStreamSynchronize(s));
+  }
+  *t = c->ctl_host->t;
+  *dt_cur = c->ctl_host->dt_cur;
+  fill_stats(c, st);
+  return c->ctl_host->status;
+}
+
+static void host_field(const tdgl_field* f, double t, double& bx, double& by, double& bz) {
+  if (f->constant) { bx = f->Bx; by = f->By; bz = f->Bz; return; }
+  if (t <= 0.0 || t > f->t_field_stop * f->t_on_fraction) { bx = by = bz = 0.0; return; }
+  double sc = 1.0;
+  if (f->ramp) {
+    double tr = f->t_field_stop * f->ramp_fraction;
+    sc = tr > 0.0 ? std::min(t / tr, 1.0) : 1.0;
+  }
+  bx = f->Bx * sc; by = f->By * sc; bz = f->Bz * sc;
+}
+
+extern "C" int tdgl_euler_run(tdgl_ctx* c, double* x, double* t, double t_stop, double dt, int32_t n_steps,
+                              const tdgl_field* f, tdgl_stream_t s) {
+  if (!c || !x || !t || !f) return fail(TDGL_EINVAL, "null argument");
+  double* a = x;
+  double* b = c->s_x;
+  for (int i = 0; i < n_steps; ++i) {
+    double dta = std::min(dt, t_stop - *t);
+    double bx, by, bz;
+    host_field(f, *t, bx, by, bz);
+    k_euler<<<grid_1d(c, c->g.n), kThreads, 0, s>>>(c->g, a, b, dta, bterms(c->g, bx, by, bz));
+    TDGL_CUDA(cudaGetLastError());
+    std::swap(a, b);
+    *t += dta;
+  }
+  if (a != x) TDGL_CUDA(cudaMemcpyAsync(x, a, c->L * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  return TDGL_OK;
+}

@@ -1,0 +1,204 @@
+"""Parity of the CUDA path (through the C ABI) with the reference's golden
+vectors and with the oracle.  Tolerances:
+
+* RHS, pack/unpack, observables: FP64, 1e-12 relative (summation order only);
+  the layout permutation is bit-exact.
+* TGCR / Newton: the reference's finite-difference product, GCR with CGS
+  instead of MGS (identical in exact arithmetic): 1e-6 relative on the
+  solution, identical iteration counts and convergence flags.
+* Trajectories: Newton tolerance level, 1e-7 absolute on the state.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import device_from_fixture, golden, golden_names
+
+pytestmark = pytest.mark.gpu
+
+CASES = golden_names("case_")
+TRAPS = [n for n in golden_names("trap_") if n != "trap_config1"]
+
+
+@pytest.fixture(scope="module")
+def tb():
+    import nanowire_tdgl_b200 as tb
+    assert torch.cuda.is_available()
+    return tb
+
+
+def _rel(a, b):
+    return np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300)
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_eval_f_matches_reference(tb, name):
+    d = golden(name)
+    dev = device_from_fixture(d)
+    u = tb.BoundaryVectors(d["u_Bx"], d["u_By"], d["u_Bz"])
+    F = tb.eval_f(d["X_seeded"], dev.params, dev.idx, u, material=dev.material)
+    assert _rel(F, d["F_seeded"]) < 1e-12
+    if "X_random" in d:
+        F = tb.eval_f(d["X_random"], dev.params, dev.idx, u, material=dev.material)
+        assert _rel(F, d["F_random"]) < 1e-12
+
+
+@pytest.mark.parametrize("name", ["case_3d_hole_edge", "case_2d_hole_triangle", "case_config1"])
+def test_pack_unpack_bit_exact(tb, name):
+    from nanowire_tdgl_b200.engine import grid_for
+    d = golden(name)
+    dev = device_from_fixture(d)
+    g = grid_for(dev.params, dev.idx, dev.material)
+    X = d["X_seeded"]
+    back = g.unpack(g.pack(X)).cpu().numpy()
+    assert np.array_equal(back, X)
+
+
+@pytest.mark.parametrize("name", ["case_3d_basic", "case_3d_hole", "case_trilayer", "case_2d_basic"])
+def test_jvp_matches_central_difference(tb, name):
+    from nanowire_tdgl_b200.engine import grid_for
+    from oracle import tdgl_oracle as orc
+    d = golden(name)
+    dev = device_from_fixture(d)
+    og = orc.make_grid(dev.params, dev.idx, dev.material)
+    g = grid_for(dev.params, dev.idx, dev.material)
+    X = d.get("X_random", d["X_seeded"])
+    rng = np.random.default_rng(2)
+    P = rng.standard_normal(dev.params.n_state) + 0j
+    dt, h = 0.1, 1e-5
+    fd = (orc.eval_f(X + h * P, og, *d["B"]) - orc.eval_f(X - h * P, og, *d["B"])) / (2 * h)
+    want = P - dt / 2 * fd
+    ap = g.unpack(g.jvp(g.pack(X), g.pack(P), dt, "analytic", B=d["B"])).cpu().numpy()
+    assert _rel(ap, want) < 1e-8
+    ap_fd = g.unpack(g.jvp(g.pack(X), g.pack(P), dt, "fd", 1e-4, B=d["B"])).cpu().numpy()
+    assert _rel(ap_fd, want) < 1e-3
+
+
+@pytest.mark.parametrize("name", ["solver_3d_basic", "solver_3d_hole", "solver_2d_basic"])
+def test_tgcr_and_newton_match_reference(tb, name):
+    d = golden(name)
+    case = golden("case_" + name[len("solver_"):])
+    dev = device_from_fixture(case)
+    f = tb.make_eval_f(dev.params, dev.idx, tuple(case["B"]), dev.material)
+    dt = float(d["dt"])
+    x = tb.tgcr_matrix_free_trap(f, d["x_lin"], d["b"], dt, tol=float(d["tgcr_tol"]))
+    assert x.size and _rel(x, d["tgcr_x"]) < 1e-6
+    xn, ok, it = tb.newton_gcr_trap(f, d["x_pred"], d["gamma"], dt, tol_f=1e-8, tol_dx=1e-3, max_iter=20,
+                                    tol_gcr=1e-6)
+    assert ok == bool(d["newton_converged"]) and it == int(d["newton_iters"])
+    assert np.max(np.abs(xn - d["newton_x"])) < 1e-8
+
+
+def test_tgcr_edge_cases(tb):
+    d = golden("case_3d_basic")
+    dev = device_from_fixture(d)
+    f = tb.make_eval_f(dev.params, dev.idx, (0.0, 0.0, 0.0), dev.material)
+    X = d["X_seeded"]
+    b = 0.01 * d["X_random"]
+    assert tb.tgcr_matrix_free_trap(f, X, b, 0.1, max_iter=0).size == 0           # no iteration allowed
+    z = tb.tgcr_matrix_free_trap(f, X, np.zeros_like(b), 0.1)                        # b == 0
+    assert z.size == b.size and not np.any(z)
+    ident = tb.tgcr_matrix_free_trap(f, X, b, 0.0, tol=1e-8)                         # dt = 0: identity
+    assert np.max(np.abs(ident - b)) < 1e-12 * np.max(np.abs(b)) + 1e-18
+
+
+@pytest.mark.parametrize("name", TRAPS)
+@pytest.mark.parametrize("jvp", ["fd", "analytic"])
+def test_trapezoidal_matches_reference(tb, name, jvp):
+    d = golden(name)
+    case = golden("case_" + name[len("trap_"):])
+    dev = device_from_fixture(case)
+    sol = tb.solve(dev, t_start=0.0, t_stop=float(d["t_stop"]), dt=float(d["dt"]), method="trapezoidal",
+                   x0=d["x0"], progress=False, log_metadata=False, newton_tol_f=1e-8, newton_tol_dx=1e-3,
+                   tol_gcr=1e-6, jvp=jvp)
+    assert np.array_equal(sol.times, d["times"])
+    err = np.max(np.abs(sol.states[:, d["saved_steps"]] - d["states"]))
+    assert err < 1e-7, err
+
+
+def test_trapezoidal_config1_101_steps(tb):
+    d = golden("trap_config1")
+    case = golden("case_config1")
+    dev = device_from_fixture(case)
+    sol = tb.solve(dev, t_start=0.0, t_stop=float(d["t_stop"]), dt=float(d["dt"]), method="trapezoidal",
+                   x0=d["x0"], progress=False, log_metadata=False, newton_tol_f=1e-8, newton_tol_dx=1e-3,
+                   tol_gcr=1e-6)
+    assert len(sol.times) == 102 and np.array_equal(sol.times, d["times"])
+    err = np.max(np.abs(sol.states[:, d["saved_steps"]] - d["states"]))
+    assert err < 1e-7, err
+    # observables of the final state, as the reference's Solution computes them
+    assert np.allclose(sol.psi_squared(-1), d["psi2"], rtol=0, atol=1e-7)
+    for mine, ref in zip(sol.bfield(-1), (d["Bx"], d["By"], d["Bz"])):
+        assert np.allclose(mine, ref, rtol=0, atol=1e-6)
+    for mine, ref in zip(sol.supercurrent_density(-1), (d["Jx"], d["Jy"], d["Jz"])):
+        assert np.allclose(mine, ref, rtol=0, atol=1e-7)
+
+
+@pytest.mark.parametrize("name", TRAPS)
+def test_observables_match_reference(tb, name):
+    d = golden(name)
+    case = golden("case_" + name[len("trap_"):])
+    dev = device_from_fixture(case)
+    sol = tb.Solution(times=d["times"], states=d["states"], params=dev.params, idx=dev.idx, device=dev)
+    assert np.allclose(sol.psi_squared(-1), d["psi2"], rtol=0, atol=1e-14)
+    for mine, ref in zip(sol.bfield(-1), (d["Bx"], d["By"], d["Bz"])):
+        assert np.allclose(mine, ref, rtol=0, atol=1e-12)
+    for mine, ref in zip(sol.supercurrent_density(-1), (d["Jx"], d["Jy"], d["Jz"])):
+        assert np.allclose(mine, ref, rtol=0, atol=1e-13)
+
+
+def test_forward_euler_matches_reference(tb):
+    d = golden("euler_3d_hole")
+    case = golden("case_3d_hole")
+    dev = device_from_fixture(case)
+    sol = tb.solve(dev, t_start=0.0, t_stop=float(d["t_stop"]), dt=float(d["dt"]), method="euler",
+                   x0=d["x0"], progress=False, log_metadata=False)
+    assert np.allclose(sol.times, d["times"], rtol=0, atol=1e-15)
+    assert _rel(sol.states[:, d["saved_steps"]], d["states"]) < 1e-11
+
+
+def test_mixed_precision_against_fp64(tb):
+    d = golden("trap_config1")
+    case = golden("case_config1")
+    dev = device_from_fixture(case)
+    kw = dict(t_start=0.0, t_stop=2.0, dt=0.1, method="trapezoidal", x0=d["x0"], progress=False,
+              log_metadata=False, newton_tol_f=1e-8, newton_tol_dx=1e-3, tol_gcr=1e-6, save_every=20)
+    ref = tb.solve(dev, precision="fp64", **kw)
+    mix = tb.solve(dev, precision="mixed", **kw)
+    p_ref = np.abs(ref.psi(-1)) ** 2
+    p_mix = np.abs(mix.psi(-1)) ** 2
+    assert np.linalg.norm(p_mix - p_ref) / np.linalg.norm(p_ref) < 1e-6
+
+
+def test_dt_min_and_nonconvergence_errors(tb):
+    d = golden("case_3d_basic")
+    dev = device_from_fixture(d)
+    with pytest.raises(RuntimeError, match="dt reduced below dt_min"):
+        tb.trapezoidal(d["X_seeded"], dev.params, dev.idx, tb.FieldSchedule(dev.applied_field, dev.params,
+                       dev.idx, 1.0), 0.0, 1.0, 0.1, newton_max_iter=0, dt_min=0.05, progress=False)
+    with pytest.raises(RuntimeError, match="Newton did not converge"):
+        tb.trapezoidal(d["X_seeded"], dev.params, dev.idx, tb.FieldSchedule(dev.applied_field, dev.params,
+                       dev.idx, 1.0), 0.0, 1.0, 0.1, newton_max_iter=0, adaptive=False, progress=False)
+
+
+def test_nonfinite_state_is_reported(tb):
+    from nanowire_tdgl_b200._lib import TDGLError
+    d = golden("case_3d_basic")
+    dev = device_from_fixture(d)
+    X = d["X_seeded"].copy()
+    X[3] = np.nan
+    with pytest.raises(TDGLError, match="non-finite"):
+        tb.trapezoidal(X, dev.params, dev.idx, tb.FieldSchedule(dev.applied_field, dev.params, dev.idx, 1.0),
+                       0.0, 1.0, 0.1, progress=False)
+
+
+def test_generic_callable_contract(tb):
+    # the reference's own solver tests use plain Python callables
+    b = np.array([1.0, 2.0], dtype=np.complex128)
+    x = tb.tgcr_matrix_free_trap(lambda v: v, np.zeros(2, dtype=np.complex128), b, dt=0.0, tol=1e-8)
+    np.testing.assert_allclose(x, b, atol=1e-5)
+    x0 = np.array([1.0, 2.0], dtype=np.complex128)
+    xs, ok, it = tb.newton_gcr_trap(lambda v: np.zeros_like(v), x0, x0.copy(), dt=1.0, tol_f=1e-6, tol_dx=1e-6)
+    assert ok
+    np.testing.assert_allclose(xs, x0, atol=1e-4)
