@@ -1,0 +1,380 @@
+#!/usr/bin/env python
+"""Benchmark: trapezoidal steps/s on the 128x128x32 holed film (one B200).
+
+Workload (the precision-form configuration): Nx=Ny=128, Nz=32 cells,
+h=0.5, kappa=2, Bz=0.5 switched on for the whole run, a centred square hole
+with vertices (24,24)-(40,40) (32x32 nodes through all 33 planes), seeded
+psi0 = 1 + 0.01 (N + iN) outside the hole, phi0 = 0; dt = 0.1, Newton
+tol_f = 1e-8, tol_dx = 1e-3, GCR tol 1e-6, eps_mf = 1e-4.  A "step" is one
+accepted trapezoidal step (predictor, Newton iterations with their GCR solves).
+
+Arms:
+  --impl ours       the device stepper (default: mixed precision, FP32 Krylov
+                    vectors / FP64 state and reductions); also times the FP64
+                    stepper on the same steps and reports the |psi|^2 error.
+  --impl reference  the CPU oracle (numpy restatement of the reference
+                    algorithm) on the host cores, same workload and metric.
+
+One JSON line on rank 0.  Under torchrun (N > 1) every rank runs an
+independent replica (the stepper does not shard); value = N * K / max time.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "trapezoidal steps/s @128²×32: mixed-FP32 vs FP64 at 1e-6 rel err; % HBM peak"
+WORKLOAD = dict(Nx=128, Ny=128, Nz=32, h=0.5, kappa=2.0, Bz=0.5, hole=[(24, 24), (40, 24), (40, 40), (24, 40)],
+                dt=0.1, tol_f=1e-8, tol_dx=1e-3, tol_gcr=1e-6, eps_mf=1e-4, seed=3, t_stop=50.0)
+WORKLOAD_NAME = ("trapezoidal step, 128x128x32-cell film (499,999 interior nodes), 32x32-node hole through "
+                 "all planes, h=0.5, kappa=2, Bz=0.5, dt=0.1, Newton tol_f 1e-8 / tol_dx 1e-3, GCR tol 1e-6")
+HBM_FALLBACK_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
+    ap.add_argument("--kmax", type=int, default=64)
+    ap.add_argument("--krylov", choices=["gmres", "gcr"], default="gmres")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison run")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-budget-s", type=float, default=150.0)
+    return ap.parse_args()
+
+
+def build_device():
+    import nanowire_tdgl_b200 as tb
+    w = WORKLOAD
+    p = tb.SimulationParameters(Nx=w["Nx"], Ny=w["Ny"], Nz=w["Nz"], hx=w["h"], hy=w["h"], hz=w["h"],
+                                kappa=w["kappa"])
+    dev = tb.Device(p, applied_field=tb.AppliedField(Bz=w["Bz"], t_on_fraction=1.0))
+    dev.add_hole(w["hole"])
+    rng = np.random.default_rng(w["seed"])
+    x0 = dev.initial_state()
+    n = p.n_interior
+    x0.psi[:] += 0.01 * (rng.standard_normal(n) + 1j * rng.standard_normal(n)) * dev.material.interior_sc_mask
+    return dev, x0.data.copy()
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            v = json.load(fh).get("hbm_gbs")
+        if v:
+            return float(v), "measured"
+    except (OSError, ValueError):
+        pass
+    return HBM_FALLBACK_GBS, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# algorithmic bytes (per-stage compulsory traffic, stage counts from the device)
+# ---------------------------------------------------------------------------
+
+def algorithmic_bytes(n_int: int, precision: str, st: dict) -> float:
+    """Compulsory HBM bytes of the counted work.
+
+    S64 = 40 B/node (psi complex + 3 real links, FP64 state), SK = bytes/node
+    of the Krylov vectors (20 B FP32 in the mixed form, 40 B FP64), F = 1 B/node
+    of flags.  Per stage:
+      RHS f(x) (predictor, Newton residual)      2 S64 + F
+      Jacobian product and A p formation         3 SK + F
+      Gram-Schmidt + alpha/x/r updates, solve of m iterations:
+                                                  sum_k (2(k-1) + 8) SK = (m^2 + 7 m) SK
+      Newton residual, norms, x += dx            7 S64 per Newton iteration
+    """
+    S64 = 40.0 * n_int
+    SK = (20.0 if precision == "mixed" else 40.0) * n_int
+    F = 1.0 * n_int
+    return (st["rhs_evals"] * (2 * S64 + F) + st["jvp_evals"] * (3 * SK + F)
+            + (st["krylov_sq"] + 7 * st["krylov_iters"]) * SK + 7 * S64 * st["newton_iters"])
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+
+class Clocks:
+    QUERY = ("index,uuid,clocks.sm,clocks.max.sm,power.draw,utilization.gpu,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self):
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                                          "-lms", "100"], stdout=self.fh, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self, uuid: str | None):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.fh.close()
+        rows = []
+        with open(self.path) as fh:
+            for line in fh:
+                f = [x.strip() for x in line.split(",")]
+                if len(f) < 11:
+                    continue
+                if uuid and uuid not in f[1]:
+                    continue
+                rows.append(f)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        def num(v):
+            try:
+                return float(v)
+            except ValueError:
+                return None
+        load = [r for r in rows if (num(r[5]) or 0) > 0] or rows
+        sm = [num(r[2]) for r in load if num(r[2]) is not None]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in load:
+            for nm, v in zip(names, r[7:11]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": num(load[0][3]),
+                "reasons": sorted(reasons), "samples": len(rows), "samples_under_load": len(load)}
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+
+def device_run(g, x0, opts, fld, warmup, steps, dist):
+    import torch
+    x = g.pack(x0)
+    t, cur = 0.0, WORKLOAD["dt"]
+    if warmup > 0:
+        rc, t, cur, _ = g.trap_run(x, t, cur, warmup, opts, fld)
+        if rc != 0:
+            raise RuntimeError(f"warm-up failed with status {rc}")
+    torch.cuda.synchronize()
+    if dist:
+        torch.distributed.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    rc, t, cur, st = g.trap_run(x, t, cur, steps, opts, fld)
+    e1.record()
+    torch.cuda.synchronize()
+    if dist:
+        torch.distributed.barrier()
+    if rc != 0 or st["steps"] != steps:
+        raise RuntimeError(f"timed run failed: status {rc}, {st['steps']} of {steps} steps")
+    return x, e0.elapsed_time(e1), st
+
+
+def run_ours(a, rank, world):
+    import torch
+    import nanowire_tdgl_b200 as tb
+    from nanowire_tdgl_b200 import _lib as L
+    from nanowire_tdgl_b200.engine import grid_for
+
+    dist = world > 1
+    dev, x0 = build_device()
+    p, w = dev.params, WORKLOAD
+    n_int = p.n_interior
+
+    def make(prec, jvp):
+        g = grid_for(p, dev.idx, dev.material, prec, a.kmax, a.krylov)
+        opts = L.TrapOpts(w["t_stop"], w["dt"], 1e-8, w["tol_f"], w["tol_dx"], w["tol_gcr"], w["eps_mf"], 20, 0, 1,
+                          L.TDGL_JVP_ANALYTIC if jvp == "analytic" else L.TDGL_JVP_FD)
+        fld = L.Field(0.0, 0.0, w["Bz"], 1.0, 0.5, w["t_stop"], 0, 0)
+        return g, opts, fld
+
+    jvp = "analytic" if a.precision == "mixed" else "fd"
+    g, opts, fld = make(a.precision, jvp)
+    clocks = Clocks()
+    clocks.start()
+    x, ms, st = device_run(g, x0, opts, fld, a.warmup, a.steps, dist)
+    uuid = None
+    try:
+        uuid = str(torch.cuda.get_device_properties(0).uuid)
+    except Exception:
+        pass
+    clk = clocks.stop(uuid)
+    ms_t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if dist:
+        torch.distributed.all_reduce(ms_t, op=torch.distributed.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+    value = world * a.steps / (ms_max / 1e3)
+
+    peak, peak_kind = measured_peak()
+    alg = algorithmic_bytes(n_int, a.precision, st)
+    achieved = alg / (ms / 1e3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "stepper_traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as fh:
+            tr = json.load(fh)
+        if tr.get("precision") == a.precision and tr.get("dram_bytes_per_step"):
+            traffic = tr["dram_bytes_per_step"] * a.steps
+    out = {
+        "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 Krylov / f64 state" if a.precision == "mixed" else "f64",
+        "data": "synthetic (seeded psi0 noise, phi0 = 0; no dataset involved)",
+        "config": {"workload": WORKLOAD_NAME, "precision": a.precision, "jvp": jvp, "krylov": a.krylov,
+                   "n_interior": n_int,
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "l2": "inputs larger than L2: Krylov basis of ~2x26 state vectors (>0.5 GB) per solve"},
+        "node_updates_per_s": value * n_int,
+        "gpu_launches": 1,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "peak_kind": peak_kind,
+                     "algorithmic_bytes_per_launch": alg, "kernel": "k_stepper (persistent, 1 launch)"},
+        "counters": {k: st[k] for k in ("newton_iters", "krylov_iters", "krylov_sq", "rhs_evals", "jvp_evals",
+                                        "rejections", "max_krylov")},
+        "clocks": clk,
+    }
+    # FP64 stepper on the same steps, and the |psi|^2 error of this run against it
+    if not a.no_fp64 and a.precision == "mixed":
+        res = {}
+        for mode in ("fd", "analytic"):
+            g64, o64, f64 = make("fp64", mode)
+            x64, ms64, st64 = device_run(g64, x0, o64, f64, a.warmup, a.steps, dist)
+            res[mode] = (x64, ms64, st64, g64)
+        x64, ms64, st64, g64 = res["fd"]
+        psi_m = g.unpack(x)[:n_int]
+        psi_d = g64.unpack(x64)[:n_int]
+        p2m, p2d = psi_m.abs() ** 2, psi_d.abs() ** 2
+        rel = float(torch.linalg.vector_norm(p2m - p2d) / torch.linalg.vector_norm(p2d))
+        out["fp64"] = {mode: {"value": a.steps / (r[1] / 1e3), "ms_per_step": r[1] / a.steps,
+                              "newton_iters": r[2]["newton_iters"], "krylov_iters": r[2]["krylov_iters"]}
+                       for mode, r in res.items()}
+        out["speedup_vs_fp64"] = {mode: out["value"] / world / v["value"] for mode, v in out["fp64"].items()}
+        out["rel_l2_psi2_vs_fp64"] = rel
+        out["max_abs_psi2_vs_fp64"] = float((p2m - p2d).abs().max())
+        out["gpu_launches"] += 0
+    # end to end through the public API: host numpy state in, every step's state back to the host
+    if not a.no_e2e:
+        sched = tb.FieldSchedule(dev.applied_field, p, dev.idx, w["t_stop"])
+        kw = dict(newton_tol_f=w["tol_f"], newton_tol_dx=w["tol_dx"], tol_gcr=w["tol_gcr"], eps_mf=w["eps_mf"],
+                  save_every=1, progress=False, material=dev.material, precision=a.precision, kmax=a.kmax,
+                  krylov=a.krylov)
+        tb.trapezoidal(x0, p, dev.idx, sched, 0.0, w["dt"], w["dt"], **kw)   # warm-up call
+        torch.cuda.synchronize()
+        if dist:
+            torch.distributed.barrier()
+        t0 = time.perf_counter()
+        times, hist = tb.trapezoidal(x0, p, dev.idx, sched, 0.0, a.steps * w["dt"], w["dt"], **kw)
+        torch.cuda.synchronize()
+        el = time.perf_counter() - t0
+        el_t = torch.tensor([el], dtype=torch.float64, device="cuda")
+        if dist:
+            torch.distributed.all_reduce(el_t, op=torch.distributed.ReduceOp.MAX)
+        el = float(el_t.item())
+        nsteps = len(times) - 1
+        sbytes = p.n_state * 16
+        out["e2e"] = {"value": world * nsteps / el, "unit": "steps/s", "h2d_bytes_per_step": sbytes / nsteps,
+                      "d2h_bytes_per_step": sbytes * (nsteps + 1) / nsteps,
+                      "call": "nanowire_tdgl_b200.trapezoidal(x0 numpy, ..., save_every=1): host state in, "
+                              "every saved state back to host memory"}
+    return out
+
+
+def cpu_oracle_steps(max_steps: int, budget_s: float, threads: int):
+    """Time the oracle's trapezoidal steps on the host (bounded by budget_s)."""
+    from threadpoolctl import threadpool_limits
+    from oracle import tdgl_oracle as orc
+    dev, x0 = build_device()
+    w = WORKLOAD
+    g = orc.make_grid(dev.params, dev.idx, dev.material)
+    fld = orc.field_schedule(Bz=w["Bz"], t_on_fraction=1.0, t_stop=w["t_stop"])
+    X = x0
+    t = 0.0
+    done = 0
+    t0 = time.perf_counter()
+    with threadpool_limits(limits=threads):
+        while done < max_steps:
+            times, hist = orc.trapezoidal(X, g, fld, t, w["t_stop"], w["dt"], newton_tol_f=w["tol_f"],
+                                          newton_tol_dx=w["tol_dx"], tol_gcr=w["tol_gcr"], eps_mf=w["eps_mf"],
+                                          max_steps=1)
+            X, t = hist[:, -1], times[-1]
+            done += 1
+            if time.perf_counter() - t0 > budget_s:
+                break
+    el = time.perf_counter() - t0
+    return done, el
+
+
+def run_reference(a, rank, world):
+    if rank != 0:
+        return None
+    cores = len(os.sched_getaffinity(0))
+    done, el = cpu_oracle_steps(a.steps, a.cpu_budget_s, cores)
+    val = done / el
+    sample = (f"{done} of {a.steps} requested trapezoidal steps from the seeded state (wall budget "
+              f"{a.cpu_budget_s:.0f} s), numpy oracle, BLAS on {cores} threads, no warm-up steps")
+    return {"metric": METRIC, "impl": "reference", "value": val, "unit": "steps/s", "n_gpus": world,
+            "steps": done, "warmup": 0, "ms_per_step": 1e3 * el / max(done, 1), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD_NAME, "precision": "fp64", "jvp": "fd"},
+            "cpu_baseline": {"value": val, "unit": "steps/s", "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": val, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    a = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if a.impl == "reference":
+        out = run_reference(a, rank, world)
+        if out is not None:
+            print(json.dumps(out), flush=True)
+        return 0
+    import torch
+    if world > 1:
+        from datetime import timedelta
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        torch.distributed.init_process_group("nccl", timeout=timedelta(seconds=300))
+    try:
+        out = run_ours(a, rank, world)
+    finally:
+        if world > 1:
+            torch.distributed.destroy_process_group()
+    if rank == 0:
+        if world == 1 and not a.no_cpu_baseline:
+            done, el = cpu_oracle_steps(1, a.cpu_budget_s, 1)
+            out["cpu_baseline"] = {"value": done / el, "unit": "steps/s", "cores": 1, "kind": "port",
+                                   "sample": f"{done} trapezoidal step(s) from the seeded state (step 1), numpy "
+                                             "oracle restating the reference algorithm, 1 thread"}
+        print(json.dumps(out), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

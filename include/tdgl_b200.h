@@ -57,6 +57,11 @@ typedef enum tdgl_jvp_mode {
   TDGL_JVP_ANALYTIC = 1  /* exact tangent-linear RHS */
 } tdgl_jvp_mode;
 
+typedef enum tdgl_krylov {
+  TDGL_KRYLOV_GMRES = 0, /* Arnoldi basis, one stored vector per iteration (default) */
+  TDGL_KRYLOV_GCR = 1    /* the reference's GCR: (p, Ap) pairs, tgcr.py:96-156 */
+} tdgl_krylov;
+
 /* Grid and physics (SimulationParameters, src/tdgl3d/core/parameters.py:10-51). */
 typedef struct tdgl_grid_desc {
   int32_t Nx, Ny, Nz;                       /* cells; Nz == 1 is the 2-D model */
@@ -105,6 +110,7 @@ typedef struct tdgl_stats {
   int32_t steps;                            /* accepted steps in this call */
   int32_t newton_converged, newton_iters_last, krylov_last, max_krylov;
   int64_t newton_iters, krylov_iters, rhs_evals, jvp_evals, rejections;
+  int64_t krylov_sq;                        /* sum over linear solves of (iterations)^2 */
   double t, dt_cur;                         /* integrator clock after the call */
   double last_gnorm, last_dxnorm;
   int64_t kernel_launches;
@@ -118,6 +124,10 @@ typedef struct tdgl_stats {
 int tdgl_ctx_create(const tdgl_grid_desc* grid, const tdgl_material_desc* material, int32_t precision,
                     int32_t kmax, tdgl_ctx** out);
 int tdgl_ctx_destroy(tdgl_ctx* ctx);
+/* Krylov method of the context's solves (tdgl_krylov).  Both minimise the
+ * residual over the same Krylov space with the reference's stopping test
+ * (tgcr.py:125, 154); GMRES stores one vector per iteration instead of two. */
+int tdgl_ctx_set_krylov(tdgl_ctx* ctx, int32_t kind);
 int64_t tdgl_n_interior(const tdgl_ctx* ctx);
 int64_t tdgl_npad(const tdgl_ctx* ctx);
 int64_t tdgl_state_len(const tdgl_ctx* ctx);        /* doubles of one device-layout state */
@@ -175,6 +185,15 @@ int tdgl_trap_run(tdgl_ctx* ctx, double* x_dev, double* t, double* dt_cur, int32
  * (src/tdgl3d/solvers/integrators.py:35-89). */
 int tdgl_euler_run(tdgl_ctx* ctx, double* x_dev, double* t, double t_stop, double dt, int32_t n_steps,
                    const tdgl_field* field, tdgl_stream_t stream);
+
+/* ---- diagnostics --------------------------------------------------------- */
+
+/* Phase timers of the persistent stepper (global-timer nanoseconds), recorded
+ * when the environment variable TDGL_PROFILE is set at context creation:
+ * out[0..15] block-0 totals per phase, out[64 + 1024 s + b] per-block compute
+ * totals of phase s (0: Krylov stencil, 1: orthogonalisation).  No reference
+ * counterpart (the reference only times whole runs, io/logging.py:284-314). */
+int tdgl_profile(tdgl_ctx* ctx, uint64_t* out, int64_t n, int32_t reset);
 
 #ifdef __cplusplus
 }

@@ -17,6 +17,7 @@ TDGL_OK, TDGL_ENOCONV, TDGL_EDTMIN, TDGL_EKMAX, TDGL_ENONFINITE, TDGL_ETIMEOUT, 
     TDGL_ENOMEM = range(9)
 TDGL_FP64, TDGL_MIXED = 0, 1
 TDGL_JVP_FD, TDGL_JVP_ANALYTIC = 0, 1
+TDGL_KRYLOV_GMRES, TDGL_KRYLOV_GCR = 0, 1
 
 
 class GridDesc(C.Structure):
@@ -48,7 +49,7 @@ class Stats(C.Structure):
     _fields_ = [("status", C.c_int32), ("steps", C.c_int32), ("newton_converged", C.c_int32),
                 ("newton_iters_last", C.c_int32), ("krylov_last", C.c_int32), ("max_krylov", C.c_int32),
                 ("newton_iters", C.c_int64), ("krylov_iters", C.c_int64), ("rhs_evals", C.c_int64),
-                ("jvp_evals", C.c_int64), ("rejections", C.c_int64), ("t", C.c_double), ("dt_cur", C.c_double),
+                ("jvp_evals", C.c_int64), ("rejections", C.c_int64), ("krylov_sq", C.c_int64), ("t", C.c_double), ("dt_cur", C.c_double),
                 ("last_gnorm", C.c_double), ("last_dxnorm", C.c_double), ("kernel_launches", C.c_int64)]
 
     def as_dict(self) -> dict:
@@ -63,6 +64,7 @@ _I = C.c_int32
 SIGNATURES = {
     "tdgl_ctx_create": (C.c_int, [C.POINTER(GridDesc), C.POINTER(MaterialDesc), _I, _I, C.POINTER(_P)]),
     "tdgl_ctx_destroy": (C.c_int, [_P]),
+    "tdgl_ctx_set_krylov": (C.c_int, [_P, _I]),
     "tdgl_n_interior": (C.c_int64, [_P]),
     "tdgl_npad": (C.c_int64, [_P]),
     "tdgl_state_len": (C.c_int64, [_P]),
@@ -80,6 +82,7 @@ SIGNATURES = {
     "tdgl_trap_run": (C.c_int, [_P, _P, C.POINTER(_D), C.POINTER(_D), _I, C.POINTER(TrapOpts), C.POINTER(Field),
                                 C.POINTER(Stats), _P]),
     "tdgl_euler_run": (C.c_int, [_P, _P, C.POINTER(_D), _D, _D, _I, C.POINTER(Field), _P]),
+    "tdgl_profile": (C.c_int, [_P, C.POINTER(C.c_uint64), C.c_int64, _I]),
 }
 
 _lib = None

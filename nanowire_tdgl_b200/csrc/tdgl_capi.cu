@@ -5,15 +5,29 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
 
 #include "tdgl_b200.h"
 #include "tdgl_geometry.h"
+#include "tdgl_kernels.cuh"
 #include "tdgl_stepper.cuh"
+#include "tdgl_graph.cuh"
 
 using namespace tdgl;
+
+namespace tdgl {
+cudaError_t stepper_occupancy_f32(size_t smem, int* occ);
+cudaError_t stepper_occupancy_f64(size_t smem, int* occ);
+cudaError_t stepper_launch_f32(StepArgs<float> A, int blocks, size_t smem, cudaStream_t s);
+cudaError_t stepper_launch_f64(StepArgs<double> A, int blocks, size_t smem, cudaStream_t s);
+cudaError_t graph_build_f32(const GArgs<float>& A, cudaGraph_t* graph, cudaGraphExec_t* exec);
+cudaError_t graph_build_f64(const GArgs<double>& A, cudaGraph_t* graph, cudaGraphExec_t* exec);
+}  // namespace tdgl
+
+static constexpr long kProfLen = 64 + 2 * 1024;
 
 namespace {
 
@@ -47,6 +61,8 @@ struct tdgl_ctx {
   uint8_t* nflags = nullptr;
   double* k2 = nullptr;
   double* sc = nullptr;
+  int* slow_off = nullptr;
+  int* slow_idx = nullptr;
   // scratch for the reference-layout operators
   double* s_x = nullptr;
   double* s_f = nullptr;
@@ -60,14 +76,35 @@ struct tdgl_ctx {
   void* XL = nullptr;
   void* P = nullptr;
   void* AP = nullptr;
+  double* hbuf = nullptr;
   double* partials = nullptr;
+  int krylov = KRY_GMRES;
   double* results = nullptr;
   unsigned* bar = nullptr;
   int* err = nullptr;
   Ctl* ctl_dev = nullptr;
   Ctl* ctl_host = nullptr;
+  unsigned long long* prof = nullptr;   // phase timers when TDGL_PROFILE is set
   int blocks = 0;
   size_t smem = 0;
+  // graph executor (GMRES trapezoidal steps)
+  bool gws_ready = false;
+  long npf = 0;             // full-grid component stride of the effective copies
+  int gblocks = 0;          // blocks of its grid kernels
+  double* Xn = nullptr;
+  double* En = nullptr;
+  double* Ei = nullptr;
+  void* XLe = nullptr;
+  void* VE = nullptr;
+  double* part_dots = nullptr;
+  double* part_orth = nullptr;
+  double* part_nrhs = nullptr;
+  double* part_upd = nullptr;
+  double* kry = nullptr;
+  GDev* gdev = nullptr;
+  GDev* gdev_host = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
   std::vector<void*> owned;
 };
 
@@ -135,6 +172,14 @@ extern "C" int tdgl_ctx_create(const tdgl_grid_desc* gd, const tdgl_material_des
     TDGL_CUDA(cudaMemcpy(c->sc, hg.sc.data(), n * sizeof(double), cudaMemcpyHostToDevice));
   }
   g.scint = c->sc;
+  if ((rc = ctx_alloc(c, (void**)&c->slow_off, hg.slow_off.size() * sizeof(int)))) { tdgl_ctx_destroy(c); return rc; }
+  TDGL_CUDA(cudaMemcpy(c->slow_off, hg.slow_off.data(), hg.slow_off.size() * sizeof(int), cudaMemcpyHostToDevice));
+  g.slow_off = c->slow_off;
+  if (!hg.slow_idx.empty()) {
+    if ((rc = ctx_alloc(c, (void**)&c->slow_idx, hg.slow_idx.size() * sizeof(int)))) { tdgl_ctx_destroy(c); return rc; }
+    TDGL_CUDA(cudaMemcpy(c->slow_idx, hg.slow_idx.data(), hg.slow_idx.size() * sizeof(int), cudaMemcpyHostToDevice));
+  }
+  g.slow_idx = c->slow_idx;
   const size_t vbytes = (size_t)c->L * sizeof(double);
   if ((rc = ctx_alloc(c, (void**)&c->s_x, vbytes))) { tdgl_ctx_destroy(c); return rc; }
   if ((rc = ctx_alloc(c, (void**)&c->s_f, vbytes))) { tdgl_ctx_destroy(c); return rc; }
@@ -147,8 +192,11 @@ extern "C" int tdgl_ctx_create(const tdgl_grid_desc* gd, const tdgl_material_des
 
 extern "C" int tdgl_ctx_destroy(tdgl_ctx* c) {
   if (!c) return TDGL_OK;
+  if (c->gexec) cudaGraphExecDestroy(c->gexec);
+  if (c->graph) cudaGraphDestroy(c->graph);
   for (void* p : c->owned) cudaFree(p);
   if (c->ctl_host) cudaFreeHost(c->ctl_host);
+  if (c->gdev_host) cudaFreeHost(c->gdev_host);
   delete c;
   return TDGL_OK;
 }
@@ -248,14 +296,10 @@ extern "C" int tdgl_observables(tdgl_ctx* c, const double* x, double Bx, double 
 // Solver workspace and the persistent launch
 // ---------------------------------------------------------------------------
 
-template <typename T>
 static int setup_launch(tdgl_ctx* c) {
-  int nacc = c->kmax + 4;
-  c->smem = (size_t)(kWarps * nacc + 2 * nacc + 3 * c->kmax) * sizeof(double);
-  if (c->smem > 48 * 1024)
-    TDGL_CUDA(cudaFuncSetAttribute(k_stepper<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem));
+  c->smem = stepper_smem(c->kmax);
   int occ = 0;
-  TDGL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stepper<T>, kThreads, c->smem));
+  TDGL_CUDA(c->precision == TDGL_MIXED ? stepper_occupancy_f32(c->smem, &occ) : stepper_occupancy_f64(c->smem, &occ));
   if (occ < 1) return fail(TDGL_ECUDA, "stepper kernel does not fit on an SM");
   c->blocks = c->num_sms * std::min(occ, 1);
   return TDGL_OK;
@@ -273,16 +317,20 @@ static int ensure_workspace(tdgl_ctx* c) {
     if ((rc = ctx_alloc(c, &c->R[i], tb))) return rc;
   if (c->precision == TDGL_MIXED)
     if ((rc = ctx_alloc(c, &c->XL, tb))) return rc;
-  if ((rc = ctx_alloc(c, &c->P, tb * c->kmax))) return rc;
+  if ((rc = ctx_alloc(c, &c->P, tb * (c->kmax + 1)))) return rc;
   if ((rc = ctx_alloc(c, &c->AP, tb * c->kmax))) return rc;
-  rc = c->precision == TDGL_MIXED ? setup_launch<float>(c) : setup_launch<double>(c);
+  rc = setup_launch(c);
   if (rc) return rc;
+  if ((rc = ctx_alloc(c, (void**)&c->hbuf, sizeof(double) * hbuf_stride(c->kmax) * (size_t)c->blocks))) return rc;
   int nslot = c->kmax + 4;
   if ((rc = ctx_alloc(c, (void**)&c->partials, sizeof(double) * nslot * (size_t)c->blocks))) return rc;
   if ((rc = ctx_alloc(c, (void**)&c->results, sizeof(double) * nslot))) return rc;
   if ((rc = ctx_alloc(c, (void**)&c->bar, 4 * sizeof(unsigned)))) return rc;
   if ((rc = ctx_alloc(c, (void**)&c->err, 4 * sizeof(int)))) return rc;
   if ((rc = ctx_alloc(c, (void**)&c->ctl_dev, sizeof(Ctl)))) return rc;
+  const char* pe = std::getenv("TDGL_PROFILE");
+  if (pe && pe[0] && pe[0] != '0')
+    if ((rc = ctx_alloc(c, (void**)&c->prof, kProfLen * sizeof(unsigned long long)))) return rc;
   TDGL_CUDA(cudaMallocHost((void**)&c->ctl_host, sizeof(Ctl)));
   c->ws_ready = true;
   return TDGL_OK;
@@ -308,8 +356,10 @@ static StepArgs<T> make_args(tdgl_ctx* c, double* x0, double* x1, double* G, dou
   A.XL = (T*)c->XL;
   A.P = (T*)c->P;
   A.AP = (T*)c->AP;
+  A.hbuf = c->hbuf;
   A.kmax = c->kmax;
   A.L = c->L;
+  A.prof = c->prof;
   return A;
 }
 
@@ -319,15 +369,10 @@ static int run_stepper(tdgl_ctx* c, double* x0, double* x1, double* G, double* D
   TDGL_CUDA(cudaMemsetAsync(c->bar, 0, 4 * sizeof(unsigned), s));
   TDGL_CUDA(cudaMemsetAsync(c->err, 0, 4 * sizeof(int), s));
   TDGL_CUDA(cudaMemcpyAsync(c->ctl_dev, c->ctl_host, sizeof(Ctl), cudaMemcpyHostToDevice, s));
-  if (c->precision == TDGL_MIXED) {
-    StepArgs<float> A = make_args<float>(c, x0, x1, G, D);
-    void* args[] = {&A};
-    TDGL_CUDA(cudaLaunchCooperativeKernel((void*)k_stepper<float>, c->blocks, kThreads, args, c->smem, s));
-  } else {
-    StepArgs<double> A = make_args<double>(c, x0, x1, G, D);
-    void* args[] = {&A};
-    TDGL_CUDA(cudaLaunchCooperativeKernel((void*)k_stepper<double>, c->blocks, kThreads, args, c->smem, s));
-  }
+  if (c->precision == TDGL_MIXED)
+    TDGL_CUDA(stepper_launch_f32(make_args<float>(c, x0, x1, G, D), c->blocks, c->smem, s));
+  else
+    TDGL_CUDA(stepper_launch_f64(make_args<double>(c, x0, x1, G, D), c->blocks, c->smem, s));
   int herr = 0;
   TDGL_CUDA(cudaMemcpyAsync(c->ctl_host, c->ctl_dev, sizeof(Ctl), cudaMemcpyDeviceToHost, s));
   TDGL_CUDA(cudaMemcpyAsync(&herr, c->err, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -350,6 +395,7 @@ static void fill_stats(const tdgl_ctx* c, tdgl_stats* st) {
   st->rhs_evals = k.rhs_evals;
   st->jvp_evals = k.jvp_evals;
   st->rejections = k.rejections;
+  st->krylov_sq = k.krylov_sq;
   st->t = k.t;
   st->dt_cur = k.dt_cur;
   st->last_gnorm = k.last_gnorm;
@@ -360,6 +406,14 @@ static void fill_stats(const tdgl_ctx* c, tdgl_stats* st) {
 static void ctl_reset(tdgl_ctx* c) {
   std::memset(c->ctl_host, 0, sizeof(Ctl));
   c->ctl_host->field_const = 1;
+  c->ctl_host->krylov = c->krylov;
+}
+
+extern "C" int tdgl_ctx_set_krylov(tdgl_ctx* c, int32_t kind) {
+  if (!c) return fail(TDGL_EINVAL, "null argument");
+  if (kind != TDGL_KRYLOV_GMRES && kind != TDGL_KRYLOV_GCR) return fail(TDGL_EINVAL, "unknown Krylov method");
+  c->krylov = kind;
+  return TDGL_OK;
 }
 
 static int krylov_cap(const tdgl_ctx* c, int32_t max_iter) {
@@ -381,8 +435,10 @@ extern "C" int tdgl_tgcr_trap(tdgl_ctx* c, const double* x_lin, const double* bv
     return fail(TDGL_EINVAL, "the finite-difference product needs the FP64 context");
   int rc;
   if ((rc = ensure_workspace(c))) return rc;
-  if (c->precision == TDGL_MIXED) k_to_t<float><<<grid_1d(c, c->L), kThreads, 0, s>>>(bvec, (float*)c->R[0], c->L);
-  else TDGL_CUDA(cudaMemcpyAsync(c->R[0], bvec, c->L * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  // the first Krylov vector: GCR keeps it in R[0], GMRES in basis slot 0
+  void* r0 = c->krylov == KRY_GCR ? c->R[0] : c->P;
+  if (c->precision == TDGL_MIXED) k_to_t<float><<<grid_1d(c, c->L), kThreads, 0, s>>>(bvec, (float*)r0, c->L);
+  else TDGL_CUDA(cudaMemcpyAsync(r0, bvec, c->L * sizeof(double), cudaMemcpyDeviceToDevice, s));
   ctl_reset(c);
   Ctl& k = *c->ctl_host;
   k.run_mode = RUN_TGCR;
@@ -423,11 +479,157 @@ extern "C" int tdgl_newton_trap(tdgl_ctx* c, double* x, const double* gamma, dou
   return c->ctl_host->status;
 }
 
+// ---------------------------------------------------------------------------
+// Graph executor (GMRES): workspace, graph, launch
+// ---------------------------------------------------------------------------
+
+template <typename T>
+static GArgs<T> make_gargs(tdgl_ctx* c) {
+  GArgs<T> A{};
+  A.g = c->g;
+  A.dev = c->gdev;
+  A.Xn = c->Xn;
+  A.Xi = c->X1;
+  A.G = c->G;
+  A.F = c->F;
+  A.En = c->En;
+  A.Ei = c->Ei;
+  A.XLe = (T*)c->XLe;
+  A.VE = (T*)c->VE;
+  A.V = (T*)c->P;
+  A.W = (T*)c->AP;
+  A.part_dots = c->part_dots;
+  A.part_orth = c->part_orth;
+  A.part_nrhs = c->part_nrhs;
+  A.part_upd = c->part_upd;
+  A.kry = c->kry;
+  A.L = c->L;
+  A.npf = c->npf;
+  A.kmax = c->kmax;
+  A.nblk = c->gblocks;
+  return A;
+}
+
+static int ensure_graph(tdgl_ctx* c) {
+  if (c->gexec) return TDGL_OK;
+  int rc;
+  if ((rc = ensure_workspace(c))) return rc;
+  const Grid& g = c->g;
+  long dimx = g.is3d ? (long)g.mk * (g.Nz + 1) : (long)g.mk;
+  c->npf = (dimx + 127) / 128 * 128;
+  c->gblocks = c->num_sms * 4;
+  const size_t tsz = c->precision == TDGL_MIXED ? sizeof(float) : sizeof(double);
+  const size_t full64 = (size_t)g.ncomp * c->npf * sizeof(double);
+  const size_t fullT = (size_t)g.ncomp * c->npf * tsz;
+  const size_t nb = (size_t)c->gblocks;
+  if ((rc = ctx_alloc(c, (void**)&c->Xn, c->L * sizeof(double)))) return rc;
+  if ((rc = ctx_alloc(c, (void**)&c->En, full64))) return rc;
+  if ((rc = ctx_alloc(c, (void**)&c->Ei, full64))) return rc;
+  if (c->precision == TDGL_MIXED) {
+    if ((rc = ctx_alloc(c, &c->XLe, fullT))) return rc;
+  } else {
+    c->XLe = c->Ei;
+  }
+  if ((rc = ctx_alloc(c, &c->VE, fullT))) return rc;
+  if ((rc = ctx_alloc(c, (void**)&c->part_dots, sizeof(double) * (c->kmax + 1) * nb))) return rc;
+  if ((rc = ctx_alloc(c, (void**)&c->part_orth, sizeof(double) * nb))) return rc;
+  if ((rc = ctx_alloc(c, (void**)&c->part_nrhs, sizeof(double) * 3 * nb))) return rc;
+  if ((rc = ctx_alloc(c, (void**)&c->part_upd, sizeof(double) * nb))) return rc;
+  if ((rc = ctx_alloc(c, (void**)&c->kry, sizeof(double) * kry_len(c->kmax)))) return rc;
+  if ((rc = ctx_alloc(c, (void**)&c->gdev, sizeof(GDev)))) return rc;
+  TDGL_CUDA(cudaMallocHost((void**)&c->gdev_host, sizeof(GDev)));
+  cudaError_t e = c->precision == TDGL_MIXED ? graph_build_f32(make_gargs<float>(c), &c->graph, &c->gexec)
+                                             : graph_build_f64(make_gargs<double>(c), &c->graph, &c->gexec);
+  if (e != cudaSuccess) {
+    if (c->graph) cudaGraphDestroy(c->graph);
+    c->graph = nullptr;
+    c->gexec = nullptr;
+    return fail(TDGL_ECUDA, std::string("building the stepper graph: ") + cudaGetErrorString(e));
+  }
+  return TDGL_OK;
+}
+
+static int graph_status(int gs) {
+  switch (gs) {
+    case GS_OK: return TDGL_OK;
+    case GS_NOCONV: return TDGL_ENOCONV;
+    case GS_DTMIN: return TDGL_EDTMIN;
+    case GS_KMAX: return TDGL_EKMAX;
+    case GS_NONFINITE: return TDGL_ENONFINITE;
+    default: return TDGL_ETIMEOUT;
+  }
+}
+
+static int run_graph(tdgl_ctx* c, double* x, double* t, double* dt_cur, int32_t max_steps, const tdgl_trap_opts* o,
+                     const tdgl_field* f, tdgl_stats* st, tdgl_stream_t s) {
+  int rc;
+  if ((rc = ensure_graph(c))) return rc;
+  GDev& h = *c->gdev_host;
+  std::memset(&h, 0, sizeof(GDev));
+  h.t = *t;
+  h.dt_cur = *dt_cur;
+  h.t_stop = o->t_stop;
+  h.dt = o->dt;
+  h.dt_min = o->dt_min;
+  h.tol_f = o->newton_tol_f;
+  h.tol_dx = o->newton_tol_dx;
+  h.tol_gcr = o->tol_gcr;
+  h.eps_mf = o->eps_mf;
+  h.Bx = f->Bx; h.By = f->By; h.Bz = f->Bz;
+  h.t_on_fraction = f->t_on_fraction;
+  h.ramp_fraction = f->ramp_fraction;
+  h.t_field_stop = f->t_field_stop;
+  h.ramp = f->ramp;
+  h.field_const = f->constant;
+  h.newton_max_iter = o->newton_max_iter;
+  h.krylov_max_iter = krylov_cap(c, o->krylov_max_iter);
+  h.adaptive = o->adaptive;
+  h.jvp_mode = o->jvp_mode;
+  h.max_steps = max_steps;
+  // hard limit on loop iterations: every step may be retried down to dt_min
+  // (at most ~12 cuts of dt/10 in double range) with full Newton / Krylov loops
+  h.watchdog_cap = (long long)(max_steps + 1) * 40 * (o->newton_max_iter + 2) * (c->kmax + 3) + 1000;
+  if (tdgl_stats* z = st) std::memset(z, 0, sizeof(*z));
+  if (!(h.t < h.t_stop - 1e-14) || max_steps <= 0) {
+    if (st) { st->t = h.t; st->dt_cur = h.dt_cur; }
+    return TDGL_OK;
+  }
+  TDGL_CUDA(cudaMemcpyAsync(c->Xn, x, c->L * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  TDGL_CUDA(cudaMemcpyAsync(c->gdev, &h, sizeof(GDev), cudaMemcpyHostToDevice, s));
+  TDGL_CUDA(cudaGraphLaunch(c->gexec, s));
+  TDGL_CUDA(cudaMemcpyAsync(&h, c->gdev, sizeof(GDev), cudaMemcpyDeviceToHost, s));
+  TDGL_CUDA(cudaMemcpyAsync(x, c->Xn, c->L * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  TDGL_CUDA(cudaStreamSynchronize(s));
+  *t = h.t;
+  *dt_cur = h.dt_cur;
+  if (st) {
+    st->status = graph_status(h.status);
+    st->steps = h.steps;
+    st->newton_converged = h.accepted;
+    st->newton_iters_last = h.newton_k;
+    st->krylov_last = h.krylov_last;
+    st->max_krylov = h.max_krylov;
+    st->newton_iters = h.newton_iters;
+    st->krylov_iters = h.krylov_iters;
+    st->krylov_sq = h.krylov_sq;
+    st->rhs_evals = h.rhs_evals;
+    st->jvp_evals = h.jvp_evals;
+    st->rejections = h.rejections;
+    st->t = h.t;
+    st->dt_cur = h.dt_cur;
+    st->last_gnorm = h.gnorm;
+    st->last_dxnorm = h.dxnorm;
+    st->kernel_launches = 1;
+  }
+  return graph_status(h.status);
+}
+
 extern "C" int tdgl_trap_run(tdgl_ctx* c, double* x, double* t, double* dt_cur, int32_t max_steps,
                              const tdgl_trap_opts* o, const tdgl_field* f, tdgl_stats* st, tdgl_stream_t s) {
   if (!c || !x || !t || !dt_cur || !o || !f) return fail(TDGL_EINVAL, "null argument");
   if (o->jvp_mode == TDGL_JVP_FD && c->precision == TDGL_MIXED)
     return fail(TDGL_EINVAL, "the finite-difference product needs the FP64 context");
+  if (c->krylov == KRY_GMRES) return run_graph(c, x, t, dt_cur, max_steps, o, f, st, s);
   int rc;
   if ((rc = ensure_workspace(c))) return rc;
   ctl_reset(c);
@@ -491,5 +693,13 @@ extern "C" int tdgl_euler_run(tdgl_ctx* c, double* x, double* t, double t_stop, 
     *t += dta;
   }
   if (a != x) TDGL_CUDA(cudaMemcpyAsync(x, a, c->L * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  return TDGL_OK;
+}
+
+extern "C" int tdgl_profile(tdgl_ctx* c, uint64_t* out, int64_t n, int32_t reset) {
+  if (!c || !c->prof) return fail(TDGL_EINVAL, "phase timers are off (set TDGL_PROFILE=1 before creating the context)");
+  int64_t m = std::min<int64_t>(n, kProfLen);
+  if (out && m > 0) TDGL_CUDA(cudaMemcpy(out, c->prof, m * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+  if (reset) TDGL_CUDA(cudaMemset(c->prof, 0, kProfLen * sizeof(uint64_t)));
   return TDGL_OK;
 }

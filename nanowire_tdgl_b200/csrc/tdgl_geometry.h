@@ -4,6 +4,7 @@
 // Plain C++ (no CUDA), shared by tdgl_ctx_create and the CPU stencil test.
 #pragma once
 
+#include <algorithm>
 #include <cstdint>
 #include <string>
 #include <vector>
@@ -19,6 +20,8 @@ struct HostGeometry {
   std::vector<uint8_t> nflags;    // interior, device order
   std::vector<double> k2;         // interior kappa^2 (empty when uniform)
   std::vector<double> sc;         // interior sc (empty unless fractional values occur)
+  std::vector<int> slow_off;      // per 128-node region offsets into slow_idx
+  std::vector<int> slow_idx;      // slow nodes grouped by region
 };
 
 inline long round_up_l(long v, long m) { return (v + m - 1) / m * m; }
@@ -123,6 +126,16 @@ inline int build_geometry(const tdgl_grid_desc* gd, const tdgl_material_desc* md
         }
         if (slow) nf[dev_of(i, j, k)] |= NF_SLOW;
       }
+  // slow nodes grouped by 128-node region (the unit of work of one warp)
+  const long nreg = g.npad / 128;
+  out.slow_off.assign(nreg + 1, 0);
+  out.slow_idx.clear();
+  for (long r = 0; r < nreg; ++r) {
+    out.slow_off[r] = (int)out.slow_idx.size();
+    for (long d = r * 128; d < std::min(n, (r + 1) * 128); ++d)
+      if (nf[d] & NF_SLOW) out.slow_idx.push_back((int)d);
+  }
+  out.slow_off[nreg] = (int)out.slow_idx.size();
   if (!any_hole) lf.clear();
   out.lflags.swap(lf);
   out.nflags.swap(nf);

@@ -1,0 +1,88 @@
+// Construction of the trapezoidal-stepper graph (see tdgl_graph.cuh): kernel
+// nodes chained linearly inside three nested conditional WHILE bodies.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "tdgl_graph.cuh"
+
+namespace tdgl {
+
+struct Chain {
+  cudaGraph_t g;
+  cudaGraphNode_t last = nullptr;
+  template <class Args>
+  cudaError_t kernel(const void* fn, int grid, int block, size_t smem, Args& args) {
+    cudaKernelNodeParams p{};
+    p.func = const_cast<void*>(fn);
+    p.gridDim = dim3(grid);
+    p.blockDim = dim3(block);
+    p.sharedMemBytes = (unsigned)smem;
+    void* a[] = {&args};
+    p.kernelParams = a;
+    cudaGraphNode_t n;
+    cudaError_t e = cudaGraphAddKernelNode(&n, g, last ? &last : nullptr, last ? 1 : 0, &p);
+    if (e == cudaSuccess) last = n;
+    return e;
+  }
+  cudaError_t loop(cudaGraphConditionalHandle h, cudaGraph_t* body) {
+    cudaGraphNodeParams p{};
+    p.type = cudaGraphNodeTypeConditional;
+    p.conditional.handle = h;
+    p.conditional.type = cudaGraphCondTypeWhile;
+    p.conditional.size = 1;
+    cudaGraphNode_t n;
+    cudaError_t e = cudaGraphAddNode(&n, g, last ? &last : nullptr, last ? 1 : 0, &p);
+    if (e == cudaSuccess) {
+      last = n;
+      *body = p.conditional.phGraph_out[0];
+    }
+    return e;
+  }
+};
+
+#define TDGL_GCK(x)                      \
+  do {                                   \
+    cudaError_t e_ = (x);                \
+    if (e_ != cudaSuccess) return e_;    \
+  } while (0)
+
+template <typename T, bool D3>
+cudaError_t build_trap_graph(GArgs<T> A, cudaGraph_t* out_graph, cudaGraphExec_t* out_exec) {
+  cudaGraph_t G;
+  TDGL_GCK(cudaGraphCreate(&G, 0));
+  *out_graph = G;
+  TDGL_GCK(cudaGraphConditionalHandleCreate(&A.h_step, G, 1, cudaGraphCondAssignDefault));
+  TDGL_GCK(cudaGraphConditionalHandleCreate(&A.h_newton, G, 0, 0));
+  TDGL_GCK(cudaGraphConditionalHandleCreate(&A.h_krylov, G, 0, 0));
+  const int nb = A.nblk;
+  const size_t fin_smem = (size_t)(A.kmax + 1) * sizeof(double);
+  Chain top{G};
+  cudaGraph_t step_body, newton_body, krylov_body;
+  TDGL_GCK(top.loop(A.h_step, &step_body));
+  Chain cs{step_body};
+  TDGL_GCK(cs.kernel((const void*)kg_step_begin<T>, 1, kThreads, 0, A));
+  TDGL_GCK(cs.kernel((const void*)kg_prepare<T, D3>, nb, kThreads, 0, A));
+  TDGL_GCK(cs.kernel((const void*)kg_predict<T, D3>, nb, kThreads, 0, A));
+  TDGL_GCK(cs.kernel((const void*)kg_newton_rhs<T, D3>, nb, kThreads, 0, A));
+  TDGL_GCK(cs.kernel((const void*)kg_newton_init<T>, 1, kThreads, 0, A));
+  TDGL_GCK(cs.loop(A.h_newton, &newton_body));
+  TDGL_GCK(cs.kernel((const void*)kg_accept<T>, nb, kThreads, 0, A));
+  TDGL_GCK(cs.kernel((const void*)kg_step_end<T>, 1, kThreads, 0, A));
+  Chain cn{newton_body};
+  TDGL_GCK(cn.loop(A.h_krylov, &krylov_body));
+  TDGL_GCK(cn.kernel((const void*)kg_newton_solve<T>, 1, kThreads, 0, A));
+  TDGL_GCK(cn.kernel((const void*)kg_update<T, D3>, nb, kThreads, 0, A));
+  TDGL_GCK(cn.kernel((const void*)kg_newton_rhs<T, D3>, nb, kThreads, 0, A));
+  TDGL_GCK(cn.kernel((const void*)kg_newton_check<T>, 1, kThreads, 0, A));
+  Chain ck{krylov_body};
+  TDGL_GCK(ck.kernel((const void*)kg_stencil<T, D3>, nb, kThreads, 0, A));
+  TDGL_GCK(ck.kernel((const void*)kg_dots<T>, nb, kThreads, 0, A));
+  TDGL_GCK(ck.kernel((const void*)kg_fin_dots<T>, 1, kThreads, fin_smem, A));
+  TDGL_GCK(ck.kernel((const void*)kg_orth<T, D3>, nb, kThreads, 0, A));
+  TDGL_GCK(ck.kernel((const void*)kg_fin_orth<T>, 1, kThreads, 0, A));
+  TDGL_GCK(cudaGraphInstantiate(out_exec, G, 0));
+  return cudaSuccess;
+}
+
+}  // namespace tdgl

@@ -1,17 +1,13 @@
-// Kernels of the device stepper: layout conversion, RHS / JVP passes,
-// observables, and the persistent trapezoidal Newton-Krylov kernel.
+// Standalone kernels: layout conversion, RHS / Jacobian products, observables,
+// forward Euler.
 #pragma once
 
 #include <cstdint>
 #include <cuda_runtime.h>
 
-#include "tdgl_stencil.cuh"
-#include "tdgl_sync.cuh"
+#include "tdgl_common.cuh"
 
 namespace tdgl {
-
-constexpr int kThreads = 512;          // threads per block of every kernel here
-constexpr int kWarps = kThreads / 32;
 
 // ---------------------------------------------------------------------------
 // Layout conversion between the reference state (complex128, interior nodes in

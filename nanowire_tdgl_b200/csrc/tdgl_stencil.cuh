@@ -70,6 +70,8 @@ struct Grid {
   const uint8_t* nflags;   // interior node flags, device order
   const double* k2int;     // kappa^2 per interior node (device order) or nullptr
   const double* scint;     // sc per interior node (device order) or nullptr
+  const int* slow_off;     // per 128-node region: offsets into slow_idx (nregions + 1)
+  const int* slow_idx;     // nodes with NF_SLOW, grouped by region, ascending
 };
 
 // Applied-field offsets of the tangential face links, in the reference's
@@ -238,15 +240,16 @@ TDGL_HD NodeCoef<T> node_coef(const Grid& g, int d, uint8_t nf) {
 // RHS at one interior node: out[PR..AZ] = dX/dt.
 // ---------------------------------------------------------------------------
 
-template <typename T, class A>
+template <typename T, bool D3, class A>
 TDGL_HD void rhs_body(const Grid& g, const A& X, const NodeCoef<T>& nc, uint8_t nf, T out[5]) {
   T cr, ci;
   X.psi(0, 0, 0, cr, ci);
-  const bool d3 = g.is3d;
-  T sup[3];
+  constexpr bool d3 = D3;
+  T sup[3] = {T(0), T(0), T(0)};
   T dre = T(0), dim = T(0);
   // gauge-covariant psi Laplacian and the supercurrent along each axis
-  for (int a = 0; a < (d3 ? 3 : 2); ++a) {
+#pragma unroll
+  for (int a = 0; a < (D3 ? 3 : 2); ++a) {
     int ex = a == 0, ey = a == 1, ez = a == 2;
     T pmr, pmi, ppr, ppi;
     X.psi(-ex, -ey, -ez, pmr, pmi);
@@ -289,7 +292,7 @@ TDGL_HD void rhs_body(const Grid& g, const A& X, const NodeCoef<T>& nc, uint8_t 
   T dfy = T(-2) * (cx + T(2) * cy + cz) * fy0 + cx * (fyxm + fyxp) + T(2) * cy * (fyym + fyyp)
           + sup[1] + cx * (-fxyp + fx0 + fxypxm - fxxm);
   T dfz = T(0);
-  if (d3) {
+  if constexpr (D3) {
     T fxzm = X.phi(0, 0, 0, -1), fxzp = X.phi(0, 0, 0, 1);
     T fyzm = X.phi(1, 0, 0, -1), fyzp = X.phi(1, 0, 0, 1);
     T fz0 = X.phi(2, 0, 0, 0), fzxm = X.phi(2, -1, 0, 0), fzxp = X.phi(2, 1, 0, 0);
@@ -316,15 +319,16 @@ TDGL_HD void rhs_body(const Grid& g, const A& X, const NodeCoef<T>& nc, uint8_t 
 // boundary maps are affine, so their tangent drops the field offsets).
 // ---------------------------------------------------------------------------
 
-template <typename T, class AXs, class APs>
+template <typename T, bool D3, class AXs, class APs>
 TDGL_HD void jvp_body(const Grid& g, const AXs& X, const APs& P, const NodeCoef<T>& nc, uint8_t nf, T out[5]) {
   T cr, ci, dcr, dci;
   X.psi(0, 0, 0, cr, ci);
   P.psi(0, 0, 0, dcr, dci);
-  const bool d3 = g.is3d;
-  T dsup[3];
+  constexpr bool d3 = D3;
+  T dsup[3] = {T(0), T(0), T(0)};
   T dre = T(0), dim = T(0);
-  for (int a = 0; a < (d3 ? 3 : 2); ++a) {
+#pragma unroll
+  for (int a = 0; a < (D3 ? 3 : 2); ++a) {
     int ex = a == 0, ey = a == 1, ez = a == 2;
     T pmr, pmi, ppr, ppi, qmr, qmi, qpr, qpi;
     X.psi(-ex, -ey, -ez, pmr, pmi);
@@ -376,7 +380,7 @@ TDGL_HD void jvp_body(const Grid& g, const AXs& X, const APs& P, const NodeCoef<
   T dfy = T(-2) * (cx + T(2) * cy + cz) * fy0 + cx * (fyxm + fyxp) + T(2) * cy * (fyym + fyyp)
           + dsup[1] + cx * (-fxyp + fx0 + fxypxm - fxxm);
   T dfz = T(0);
-  if (d3) {
+  if constexpr (D3) {
     T fxzm = P.phi(0, 0, 0, -1), fxzp = P.phi(0, 0, 0, 1);
     T fyzm = P.phi(1, 0, 0, -1), fyzp = P.phi(1, 0, 0, 1);
     T fz0 = P.phi(2, 0, 0, 0), fzxm = P.phi(2, -1, 0, 0), fzxp = P.phi(2, 1, 0, 0);
@@ -411,38 +415,62 @@ TDGL_HD void node_ijk(const Grid& g, int d, int& i, int& j, int& k) {
   }
 }
 
-// Full RHS at node d from source s (boundary rules with field offsets b).
+// RHS at node d from source s.  _fast: every neighbour is plain interior data
+// (node flag NF_SLOW clear); _slow: neighbours through the boundary rules.
+template <typename T, bool D3, class Src>
+TDGL_HD void rhs_fast(const Grid& g, const Src& s, int d, uint8_t nf, T out[5]) {
+  NodeCoef<T> nc = node_coef<T>(g, d, nf);
+  NbFast<T, Src> A{s, d, g.nx, g.nx * g.ny};
+  rhs_body<T, D3>(g, A, nc, nf, out);
+}
+template <typename T, bool D3, class Src>
+TDGL_HD void rhs_slow(const Grid& g, const Src& s, const BTerms<T>& b, int d, uint8_t nf, T out[5]) {
+  NodeCoef<T> nc = node_coef<T>(g, d, nf);
+  int i, j, k;
+  node_ijk(g, d, i, j, k);
+  NbSlow<T, Src> A{Ext<T, Src>{&g, s, b}, i, j, k};
+  rhs_body<T, D3>(g, A, nc, nf, out);
+}
 template <typename T, class Src>
 TDGL_HD void rhs_at(const Grid& g, const Src& s, const BTerms<T>& b, int d, T out[5]) {
   uint8_t nf = g.nflags[d];
-  NodeCoef<T> nc = node_coef<T>(g, d, nf);
-  if (!(nf & NF_SLOW)) {
-    NbFast<T, Src> A{s, d, g.nx, g.nx * g.ny};
-    rhs_body<T>(g, A, nc, nf, out);
+  if (g.is3d) {
+    if (nf & NF_SLOW) rhs_slow<T, true>(g, s, b, d, nf, out);
+    else rhs_fast<T, true>(g, s, d, nf, out);
   } else {
-    int i, j, k;
-    node_ijk(g, d, i, j, k);
-    NbSlow<T, Src> A{Ext<T, Src>{&g, s, b}, i, j, k};
-    rhs_body<T>(g, A, nc, nf, out);
+    if (nf & NF_SLOW) rhs_slow<T, false>(g, s, b, d, nf, out);
+    else rhs_fast<T, false>(g, s, d, nf, out);
   }
 }
 
 // Tangent RHS at node d: out = J(x) p.
+template <typename T, bool D3, class SrcX, class SrcP>
+TDGL_HD void jvp_fast(const Grid& g, const SrcX& sx, const SrcP& sp, int d, uint8_t nf, T out[5]) {
+  NodeCoef<T> nc = node_coef<T>(g, d, nf);
+  NbFast<T, SrcX> AX_{sx, d, g.nx, g.nx * g.ny};
+  NbFast<T, SrcP> AP_{sp, d, g.nx, g.nx * g.ny};
+  jvp_body<T, D3>(g, AX_, AP_, nc, nf, out);
+}
+template <typename T, bool D3, class SrcX, class SrcP>
+TDGL_HD void jvp_slow(const Grid& g, const SrcX& sx, const BTerms<T>& b, const SrcP& sp, int d, uint8_t nf,
+                      T out[5]) {
+  NodeCoef<T> nc = node_coef<T>(g, d, nf);
+  int i, j, k;
+  node_ijk(g, d, i, j, k);
+  BTerms<T> zero{T(0), T(0), T(0)};
+  NbSlow<T, SrcX> AX_{Ext<T, SrcX>{&g, sx, b}, i, j, k};
+  NbSlow<T, SrcP> AP_{Ext<T, SrcP>{&g, sp, zero}, i, j, k};
+  jvp_body<T, D3>(g, AX_, AP_, nc, nf, out);
+}
 template <typename T, class SrcX, class SrcP>
 TDGL_HD void jvp_at(const Grid& g, const SrcX& sx, const BTerms<T>& b, const SrcP& sp, int d, T out[5]) {
   uint8_t nf = g.nflags[d];
-  NodeCoef<T> nc = node_coef<T>(g, d, nf);
-  if (!(nf & NF_SLOW)) {
-    NbFast<T, SrcX> AX_{sx, d, g.nx, g.nx * g.ny};
-    NbFast<T, SrcP> AP_{sp, d, g.nx, g.nx * g.ny};
-    jvp_body<T>(g, AX_, AP_, nc, nf, out);
+  if (g.is3d) {
+    if (nf & NF_SLOW) jvp_slow<T, true>(g, sx, b, sp, d, nf, out);
+    else jvp_fast<T, true>(g, sx, sp, d, nf, out);
   } else {
-    int i, j, k;
-    node_ijk(g, d, i, j, k);
-    BTerms<T> zero{T(0), T(0), T(0)};
-    NbSlow<T, SrcX> AX_{Ext<T, SrcX>{&g, sx, b}, i, j, k};
-    NbSlow<T, SrcP> AP_{Ext<T, SrcP>{&g, sp, zero}, i, j, k};
-    jvp_body<T>(g, AX_, AP_, nc, nf, out);
+    if (nf & NF_SLOW) jvp_slow<T, false>(g, sx, b, sp, d, nf, out);
+    else jvp_fast<T, false>(g, sx, sp, d, nf, out);
   }
 }
 

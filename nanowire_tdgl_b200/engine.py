@@ -17,6 +17,7 @@ from . import _lib as L
 
 PRECISIONS = {"fp64": L.TDGL_FP64, "mixed": L.TDGL_MIXED}
 JVP_MODES = {"fd": L.TDGL_JVP_FD, "analytic": L.TDGL_JVP_ANALYTIC}
+KRYLOV = {"gmres": L.TDGL_KRYLOV_GMRES, "gcr": L.TDGL_KRYLOV_GCR}
 
 
 def _require_cuda() -> torch.device:
@@ -70,7 +71,8 @@ def descriptors(params, idx, material=None):
 class DeviceGrid:
     """Device description of one grid with its holes and material map."""
 
-    def __init__(self, params, idx, material=None, precision: str = "fp64", kmax: int = 64):
+    def __init__(self, params, idx, material=None, precision: str = "fp64", kmax: int = 64,
+                 krylov: str = "gmres"):
         self.lib = L.load()
         self.device = _require_cuda()
         if precision not in PRECISIONS:
@@ -78,12 +80,16 @@ class DeviceGrid:
         self.params = params
         self.precision = precision
         self.kmax = int(kmax)
+        if krylov not in KRYLOV:
+            raise ValueError(f"krylov must be one of {sorted(KRYLOV)}")
+        self.krylov = krylov
         g, md, keep = descriptors(params, idx, material)
         h = C.c_void_p()
         with torch.cuda.device(self.device):
             L.check(self.lib.tdgl_ctx_create(C.byref(g), C.byref(md), PRECISIONS[precision], self.kmax,
                                              C.byref(h)), "tdgl_ctx_create")
         self.handle = h
+        L.check(self.lib.tdgl_ctx_set_krylov(h, KRYLOV[krylov]), "tdgl_ctx_set_krylov")
         self.n = int(self.lib.tdgl_n_interior(h))
         self.npad = int(self.lib.tdgl_npad(h))
         self.state_len = int(self.lib.tdgl_state_len(h))
@@ -186,14 +192,15 @@ class DeviceGrid:
 _CACHE: dict = {}
 
 
-def grid_for(params, idx, material=None, precision: str = "fp64", kmax: int = 64) -> DeviceGrid:
+def grid_for(params, idx, material=None, precision: str = "fp64", kmax: int = 64,
+             krylov: str = "gmres") -> DeviceGrid:
     """Cached :class:`DeviceGrid` for these objects (keyed by identity and by
     the hole / material contents, so a device modified after first use is
     rebuilt)."""
     def sig(a):
         a = np.asarray(a)
         return (a.shape, hash(a.tobytes())) if a.size else (a.shape, 0)
-    key = (id(params), id(idx), id(material), precision, int(kmax),
+    key = (id(params), id(idx), id(material), precision, int(kmax), krylov,
            (params.Nx, params.Ny, params.Nz, params.hx, params.hy, params.hz, params.kappa,
             bool(params.periodic_x), bool(params.periodic_y), bool(params.periodic_z)),
            tuple(sig(getattr(idx, f"hole_{a}_bc_mask", [])) for a in "xyz"),
@@ -203,6 +210,6 @@ def grid_for(params, idx, material=None, precision: str = "fp64", kmax: int = 64
     if g is None:
         if len(_CACHE) > 16:
             _CACHE.clear()
-        g = DeviceGrid(params, idx, material, precision, kmax)
+        g = DeviceGrid(params, idx, material, precision, kmax, krylov)
         _CACHE[key] = g
     return g

@@ -23,7 +23,9 @@ reference algorithm with the vectors on the GPU (torch) and call the
 callable for every function value.
 
 Keyword-only additions: ``precision`` ("fp64" | "mixed"), ``jvp`` ("fd" |
-"analytic") and ``kmax`` (Krylov directions held on the device).
+"analytic"), ``krylov`` ("gmres" | "gcr": the same minimal-residual iterates,
+GMRES storing one vector per iteration instead of GCR's two) and ``kmax``
+(Krylov directions held on the device).
 """
 
 from __future__ import annotations
@@ -62,12 +64,12 @@ class DeviceRHS:
     keeps the whole solve on the device."""
 
     def __init__(self, params, idx, B, material=None, precision: str = "fp64", jvp: Optional[str] = None,
-                 kmax: int = DEFAULT_KMAX):
+                 kmax: int = DEFAULT_KMAX, krylov: str = "gmres"):
         self.params, self.idx, self.material = params, idx, material
         self.B = tuple(float(b) for b in B)
         self.precision = precision
         self.jvp = jvp or ("fd" if precision == "fp64" else "analytic")
-        self.grid = grid_for(params, idx, material, precision, kmax)
+        self.grid = grid_for(params, idx, material, precision, kmax, krylov)
 
     def __call__(self, X):
         return _out(self.grid.eval_f_ref(X, self.B), X)
@@ -259,7 +261,7 @@ def trapezoidal(x0, params, idx, eval_u: Callable, t_start: float, t_stop: float
                 tol_gcr: float = 1e-4, eps_mf: float = 1e-4, save_every: int = 1, adaptive: bool = True,
                 dt_min: float = 1e-8, progress: bool = True, verbose: bool = False, material=None,
                 precision: str = "fp64", jvp: Optional[str] = None, kmax: int = DEFAULT_KMAX,
-                stats: Optional[dict] = None):
+                krylov: str = "gmres", stats: Optional[dict] = None):
     """Implicit trapezoidal integration with Newton-GCR and dt/10 retries
     (integrators.py:92-206).  Returns (times, X_history) with X_history of
     shape (n_state, n_saved), as the reference does.
@@ -270,7 +272,7 @@ def trapezoidal(x0, params, idx, eval_u: Callable, t_start: float, t_stop: float
     per step is made with the field evaluated on the host at the step's start.
     """
     jvp = jvp or ("fd" if precision == "fp64" else "analytic")
-    g = grid_for(params, idx, material, precision, kmax)
+    g = grid_for(params, idx, material, precision, kmax, krylov)
     _check_real_links(x0, params)
     x = g.pack(x0)
     opts = L.TrapOpts(float(t_stop), float(dt), float(dt_min), float(newton_tol_f), float(newton_tol_dx),
@@ -347,7 +349,8 @@ def solve(device, t_start: float = 0.0, t_stop: float = 10.0, dt: float = 0.05, 
           x0=None, *, save_every: int = 1, progress: bool = True, verbose: bool = False,
           newton_tol_f: float = 1e-3, newton_tol_dx: float = 1e-3, newton_max_iter: int = 20,
           tol_gcr: float = 1e-4, eps_mf: float = 1e-4, adaptive: bool = True, log_metadata: bool = True,
-          log_dir="logs", precision: str = "fp64", jvp: Optional[str] = None, kmax: int = DEFAULT_KMAX):
+          log_dir="logs", precision: str = "fp64", jvp: Optional[str] = None, kmax: int = DEFAULT_KMAX,
+          krylov: str = "gmres"):
     """Run a simulation and return a :class:`~nanowire_tdgl_b200.solution.Solution`
     (runner.py:40-163)."""
     from .solution import Solution
@@ -373,7 +376,7 @@ def solve(device, t_start: float = 0.0, t_stop: float = 10.0, dt: float = 0.05, 
                                newton_tol_dx=newton_tol_dx, newton_max_iter=newton_max_iter, tol_gcr=tol_gcr,
                                eps_mf=eps_mf, save_every=save_every, adaptive=adaptive, progress=progress,
                                verbose=verbose, material=material, precision=precision, jvp=jvp, kmax=kmax,
-                               stats=run_stats)
+                               krylov=krylov, stats=run_stats)
     else:
         raise ValueError(f"Unknown method {method!r}. Use 'euler' or 'trapezoidal'.")
     wall = time.perf_counter() - t0
@@ -383,7 +386,7 @@ def solve(device, t_start: float = 0.0, t_stop: float = 10.0, dt: float = 0.05, 
                 "total_steps": int(len(times)), "params": {k: getattr(params, k) for k in
                 ("Nx", "Ny", "Nz", "hx", "hy", "hz", "kappa", "periodic_x", "periodic_y", "periodic_z")},
                 "newton_tol_f": newton_tol_f, "newton_tol_dx": newton_tol_dx, "tol_gcr": tol_gcr,
-                "precision": precision, "device_counters": run_stats,
+                "precision": precision, "krylov": krylov, "device_counters": run_stats,
                 "gpu": torch.cuda.get_device_name() if torch.cuda.is_available() else None}
         path = Path(log_dir)
         path.mkdir(parents=True, exist_ok=True)

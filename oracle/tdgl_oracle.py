@@ -291,6 +291,17 @@ def _rdot(a: np.ndarray, b: np.ndarray) -> float:
     return float(np.vdot(a, b).real)
 
 
+def _axpy(a: float, x: np.ndarray, y: np.ndarray) -> None:
+    """y += a x in place (real scalar, complex vectors), via real views."""
+    yr = y.view(np.float64)
+    xr = x.view(np.float64)
+    if yr.size > 4096:
+        from scipy.linalg.blas import daxpy
+        daxpy(xr, yr, a=a)
+    else:
+        yr += a * xr
+
+
 def tgcr_trap(f: Callable, x_lin: np.ndarray, b: np.ndarray, dt: float, tol: float = 1e-4,
               max_iter: Optional[int] = None, eps_mf: float = 1e-4, stats: Optional[dict] = None):
     """GCR for (I - dt/2 J) d = b with a finite-difference J·p and modified
@@ -315,10 +326,10 @@ def tgcr_trap(f: Callable, x_lin: np.ndarray, b: np.ndarray, dt: float, tol: flo
         p = r.copy()
         eps = eps_mf * (1.0 + xnorm) / np.linalg.norm(p)
         ap = p - (dt / 2.0) * ((f(x_lin + eps * p) - f_base) / eps)
-        for pj, apj in zip(P, AP):
+        for pj, apj in zip(P, AP):          # modified Gram-Schmidt, updated in place
             beta = _rdot(ap, apj)
-            p = p - beta * pj
-            ap = ap - beta * apj
+            _axpy(-beta, pj, p)
+            _axpy(-beta, apj, ap)
         nap = np.linalg.norm(ap)
         if nap < 1e-14:
             break
@@ -327,8 +338,8 @@ def tgcr_trap(f: Callable, x_lin: np.ndarray, b: np.ndarray, dt: float, tol: flo
         P.append(p)
         AP.append(ap)
         alpha = _rdot(r, ap)
-        x = x + alpha * p
-        r = r - alpha * ap
+        _axpy(alpha, p, x)
+        _axpy(-alpha, ap, r)
         rn = np.linalg.norm(r)
     if stats is not None:
         stats["krylov_iters"] = stats.get("krylov_iters", 0) + k

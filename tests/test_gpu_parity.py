@@ -3,7 +3,7 @@ vectors and with the oracle.  Tolerances:
 
 * RHS, pack/unpack, observables: FP64, 1e-12 relative (summation order only);
   the layout permutation is bit-exact.
-* TGCR / Newton: the reference's finite-difference product, GCR with CGS
+* TGCR / Newton: the reference's finite-difference product; GCR with CGS
   instead of MGS (identical in exact arithmetic): 1e-6 relative on the
   solution, identical iteration counts and convergence flags.
 * Trajectories: Newton tolerance level, 1e-7 absolute on the state.
@@ -75,15 +75,19 @@ def test_jvp_matches_central_difference(tb, name):
     assert _rel(ap_fd, want) < 1e-3
 
 
+@pytest.mark.parametrize("krylov", ["gcr", "gmres"])
 @pytest.mark.parametrize("name", ["solver_3d_basic", "solver_3d_hole", "solver_2d_basic"])
-def test_tgcr_and_newton_match_reference(tb, name):
+def test_tgcr_and_newton_match_reference(tb, name, krylov):
     d = golden(name)
     case = golden("case_" + name[len("solver_"):])
     dev = device_from_fixture(case)
-    f = tb.make_eval_f(dev.params, dev.idx, tuple(case["B"]), dev.material)
+    f = tb.make_eval_f(dev.params, dev.idx, tuple(case["B"]), dev.material, krylov=krylov)
     dt = float(d["dt"])
     x = tb.tgcr_matrix_free_trap(f, d["x_lin"], d["b"], dt, tol=float(d["tgcr_tol"]))
-    assert x.size and _rel(x, d["tgcr_x"]) < 1e-6
+    # GCR applies the finite-difference product along the reference's own
+    # directions (agreement to rounding); GMRES along the normalised Arnoldi
+    # vectors, so the O(eps_mf) truncation of the product differs at ~1e-5
+    assert x.size and _rel(x, d["tgcr_x"]) < (1e-6 if krylov == "gcr" else 1e-4)
     xn, ok, it = tb.newton_gcr_trap(f, d["x_pred"], d["gamma"], dt, tol_f=1e-8, tol_dx=1e-3, max_iter=20,
                                     tol_gcr=1e-6)
     assert ok == bool(d["newton_converged"]) and it == int(d["newton_iters"])
@@ -104,26 +108,27 @@ def test_tgcr_edge_cases(tb):
 
 
 @pytest.mark.parametrize("name", TRAPS)
-@pytest.mark.parametrize("jvp", ["fd", "analytic"])
-def test_trapezoidal_matches_reference(tb, name, jvp):
+@pytest.mark.parametrize("jvp,krylov", [("fd", "gcr"), ("fd", "gmres"), ("analytic", "gmres")])
+def test_trapezoidal_matches_reference(tb, name, jvp, krylov):
     d = golden(name)
     case = golden("case_" + name[len("trap_"):])
     dev = device_from_fixture(case)
     sol = tb.solve(dev, t_start=0.0, t_stop=float(d["t_stop"]), dt=float(d["dt"]), method="trapezoidal",
                    x0=d["x0"], progress=False, log_metadata=False, newton_tol_f=1e-8, newton_tol_dx=1e-3,
-                   tol_gcr=1e-6, jvp=jvp)
+                   tol_gcr=1e-6, jvp=jvp, krylov=krylov)
     assert np.array_equal(sol.times, d["times"])
     err = np.max(np.abs(sol.states[:, d["saved_steps"]] - d["states"]))
     assert err < 1e-7, err
 
 
-def test_trapezoidal_config1_101_steps(tb):
+@pytest.mark.parametrize("krylov", ["gcr", "gmres"])
+def test_trapezoidal_config1_101_steps(tb, krylov):
     d = golden("trap_config1")
     case = golden("case_config1")
     dev = device_from_fixture(case)
     sol = tb.solve(dev, t_start=0.0, t_stop=float(d["t_stop"]), dt=float(d["dt"]), method="trapezoidal",
                    x0=d["x0"], progress=False, log_metadata=False, newton_tol_f=1e-8, newton_tol_dx=1e-3,
-                   tol_gcr=1e-6)
+                   tol_gcr=1e-6, krylov=krylov)
     assert len(sol.times) == 102 and np.array_equal(sol.times, d["times"])
     err = np.max(np.abs(sol.states[:, d["saved_steps"]] - d["states"]))
     assert err < 1e-7, err
