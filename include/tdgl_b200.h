@@ -186,6 +186,23 @@ int tdgl_trap_run(tdgl_ctx* ctx, double* x_dev, double* t, double* dt_cur, int32
 int tdgl_euler_run(tdgl_ctx* ctx, double* x_dev, double* t, double t_stop, double dt, int32_t n_steps,
                    const tdgl_field* field, tdgl_stream_t stream);
 
+/* ---- allocation-free operator ---------------------------------------------- */
+
+/* dX/dt of one reference-layout state (device pointers x_ref, f_ref of
+ * 2*n_state doubles each), like tdgl_eval_f, but without a context and
+ * without allocating any memory: for callers that must not call cudaMalloc
+ * when they run (a fixed device-memory budget, device memory owned by another
+ * allocator, or no tolerance for the synchronisation an allocation implies).
+ * Geometry flags and intermediates are built on the device in one static
+ * array of this library (about 8.6 MiB per GPU that loads it, held until the
+ * process exits).  Limits: 32768 interior nodes, 262144 full-grid nodes,
+ * 65536 entries per hole list; larger inputs return TDGL_EINVAL before any
+ * device work.  Calls share that array: calls that overlap on the GPU race.
+ * The first call on a device looks the array up (cudaGetSymbolAddress); make
+ * it before any stream capture.  No counterpart in the reference. */
+int tdgl_eval_f_noalloc(const tdgl_grid_desc* grid, const tdgl_material_desc* material, const double* x_ref,
+                        double* f_ref, double Bx, double By, double Bz, tdgl_stream_t stream);
+
 /* ---- diagnostics --------------------------------------------------------- */
 
 /* Phase timers of the persistent stepper (global-timer nanoseconds), recorded

@@ -135,6 +135,11 @@ extern "C" const char* tdgl_status_string(int s) {
 
 extern "C" const char* tdgl_last_error(void) { return g_last_error.c_str(); }
 
+namespace tdgl {
+// Lets the other translation units of the library report through tdgl_last_error().
+int report_error(int code, const std::string& msg) { return fail(code, msg); }
+}  // namespace tdgl
+
 extern "C" int tdgl_ctx_create(const tdgl_grid_desc* gd, const tdgl_material_desc* md, int32_t precision,
                                int32_t kmax, tdgl_ctx** out) {
   if (!gd || !out) return fail(TDGL_EINVAL, "null argument");
