@@ -205,12 +205,24 @@ int tdgl_eval_f_noalloc(const tdgl_grid_desc* grid, const tdgl_material_desc* ma
 
 /* ---- diagnostics --------------------------------------------------------- */
 
-/* Phase timers of the persistent stepper (global-timer nanoseconds), recorded
- * when the environment variable TDGL_PROFILE is set at context creation:
- * out[0..15] block-0 totals per phase, out[64 + 1024 s + b] per-block compute
- * totals of phase s (0: Krylov stencil, 1: orthogonalisation).  No reference
- * counterpart (the reference only times whole runs, io/logging.py:284-314). */
+/* Kernel and phase timers (global-timer nanoseconds), recorded when the
+ * environment variable TDGL_PROFILE is set before the solver workspace is
+ * created.  GMRES graph executor: out[k] = summed first-block-start to
+ * last-block-end time of kernel type k (0 prepare, 1 predict, 2 newton_rhs,
+ * 3 stencil, 4 projections, 5 orthogonalisation, 6 update, 7 accept, 8 Arnoldi
+ * product, 9 Arnoldi orthogonalisation, 10 Arnoldi projections), out[16 + k] =
+ * its launch count, k < 16.  Persistent
+ * executor: out[0..15] block-0 totals per phase, out[64 + 1024 s + b]
+ * per-block compute totals of phase s (0: Krylov stencil, 1:
+ * orthogonalisation).  No reference counterpart (the reference only times
+ * whole runs, io/logging.py:284-314). */
 int tdgl_profile(tdgl_ctx* ctx, uint64_t* out, int64_t n, int32_t reset);
+/* `launches` back-to-back Arnoldi steps of the GMRES graph (analytic
+ * products: orthogonalisation, product and projection kernels) outside the
+ * graph, forming basis vector ja from whatever the workspace holds, without
+ * the Krylov bookkeeping; synchronises the stream.  For timing and profiling
+ * the kernels alone.  No reference counterpart. */
+int tdgl_arnoldi_probe(tdgl_ctx* ctx, int32_t ja, int32_t launches, tdgl_stream_t stream);
 
 #ifdef __cplusplus
 }

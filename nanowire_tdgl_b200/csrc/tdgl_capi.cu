@@ -25,6 +25,8 @@ cudaError_t stepper_launch_f32(StepArgs<float> A, int blocks, size_t smem, cudaS
 cudaError_t stepper_launch_f64(StepArgs<double> A, int blocks, size_t smem, cudaStream_t s);
 cudaError_t graph_build_f32(const GArgs<float>& A, cudaGraph_t* graph, cudaGraphExec_t* exec);
 cudaError_t graph_build_f64(const GArgs<double>& A, cudaGraph_t* graph, cudaGraphExec_t* exec);
+cudaError_t arnoldi_probe_f32(const GArgs<float>& A, int launches, cudaStream_t s);
+cudaError_t arnoldi_probe_f64(const GArgs<double>& A, int launches, cudaStream_t s);
 }  // namespace tdgl
 
 static constexpr long kProfLen = 64 + 2 * 1024;
@@ -103,8 +105,18 @@ struct tdgl_ctx {
   double* kry = nullptr;
   GDev* gdev = nullptr;
   GDev* gdev_host = nullptr;
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t gexec = nullptr;
+  cudaGraph_t graph[2] = {nullptr, nullptr};        // [0]: finite-difference Krylov body, [1]: analytic
+  cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+  bool gprof = false;                               // per-kernel timers of the graph (TDGL_PROFILE)
+  unsigned long long gk_total[kKTypes] = {};
+  long long gk_count[kKTypes] = {};
+  // Arnoldi workspace of the analytic-product graph (allocated with it)
+  void* UB = nullptr;
+  void* Zb[2] = {nullptr, nullptr};
+  double* part_arn = nullptr;
+  unsigned* ticket = nullptr;
+  int nblk_arn = 0, nblk_orth = 0, arn_gx = 0, arn_gy = 0;
+  uint8_t* imask = nullptr;
   std::vector<void*> owned;
 };
 
@@ -197,8 +209,10 @@ extern "C" int tdgl_ctx_create(const tdgl_grid_desc* gd, const tdgl_material_des
 
 extern "C" int tdgl_ctx_destroy(tdgl_ctx* c) {
   if (!c) return TDGL_OK;
-  if (c->gexec) cudaGraphExecDestroy(c->gexec);
-  if (c->graph) cudaGraphDestroy(c->graph);
+  for (int v = 0; v < 2; ++v) {
+    if (c->gexec[v]) cudaGraphExecDestroy(c->gexec[v]);
+    if (c->graph[v]) cudaGraphDestroy(c->graph[v]);
+  }
   for (void* p : c->owned) cudaFree(p);
   if (c->ctl_host) cudaFreeHost(c->ctl_host);
   if (c->gdev_host) cudaFreeHost(c->gdev_host);
@@ -512,43 +526,102 @@ static GArgs<T> make_gargs(tdgl_ctx* c) {
   A.npf = c->npf;
   A.kmax = c->kmax;
   A.nblk = c->gblocks;
+  A.UB = (T*)c->UB;
+  A.Zb[0] = (T*)c->Zb[0];
+  A.Zb[1] = (T*)c->Zb[1];
+  A.vs = (long)c->g.ncomp * c->npf;
+  A.part_arn = c->part_arn;
+  A.ticket = c->ticket;
+  A.nblk_arn = c->nblk_arn;
+  A.nblk_orth = c->nblk_orth;
+  A.arn_gx = c->arn_gx;
+  A.arn_gy = c->arn_gy;
+  A.imask = c->imask;
+  A.cxu = c->g.kappa2 / c->g.hx2;
+  A.cyu = c->g.kappa2 / c->g.hy2;
+  A.czu = c->g.is3d ? c->g.kappa2 / c->g.hz2 : 0.0;
   return A;
 }
 
-static int ensure_graph(tdgl_ctx* c) {
-  if (c->gexec) return TDGL_OK;
+// Buffers of the three-kernel Arnoldi step (analytic products).
+static int ensure_arnoldi_ws(tdgl_ctx* c) {
+  if (c->UB) return TDGL_OK;
+  const Grid& g = c->g;
+  const size_t tsz = c->precision == TDGL_MIXED ? sizeof(float) : sizeof(double);
+  const size_t vb = (size_t)g.ncomp * c->npf * tsz;
+  c->arn_gx = (g.nx + 31) / 32;
+  c->arn_gy = (g.ny + 7) / 8;
+  const char* eb = std::getenv("TDGL_DOTS_BLOCKS_PER_SM");
+  // streaming kernels of the step, resident at 5 blocks per SM (their register budgets)
+  c->nblk_arn = c->num_sms * (eb && std::atoi(eb) > 0 ? std::atoi(eb) : 5);
+  const char* eo = std::getenv("TDGL_ORTH_BLOCKS_PER_SM");
+  c->nblk_orth = std::min(c->gblocks, c->num_sms * (eo && std::atoi(eo) > 0 ? std::atoi(eo) : 5));
+  int rc;
+  if ((rc = ctx_alloc(c, &c->UB, vb * (c->kmax + 1)))) return rc;
+  if ((rc = ctx_alloc(c, &c->Zb[0], vb))) return rc;
+  if ((rc = ctx_alloc(c, &c->Zb[1], vb))) return rc;
+  if ((rc = ctx_alloc(c, (void**)&c->part_arn, sizeof(double) * (c->kmax + 2) * (size_t)c->nblk_arn))) return rc;
+  if ((rc = ctx_alloc(c, (void**)&c->ticket, sizeof(unsigned)))) return rc;
+  // interior mask of the full grid (projections run over interior entries only)
+  std::vector<uint8_t> im((size_t)c->npf, 0);
+  for (int k = g.is3d ? 1 : 0; k <= (g.is3d ? g.nz : 0); ++k)
+    for (int j = 1; j <= g.ny; ++j)
+      for (int i = 1; i <= g.nx; ++i) im[(size_t)i + (size_t)g.mj * j + (size_t)g.mk * k] = 1;
+  if ((rc = ctx_alloc(c, (void**)&c->imask, (size_t)c->npf))) return rc;
+  TDGL_CUDA(cudaMemcpy(c->imask, im.data(), (size_t)c->npf, cudaMemcpyHostToDevice));
+  return TDGL_OK;
+}
+
+// Graph variant v: 0 = finite-difference Krylov body, 1 = three-kernel Arnoldi step.
+static int ensure_graph(tdgl_ctx* c, int v) {
+  if (c->gexec[v]) return TDGL_OK;
   int rc;
   if ((rc = ensure_workspace(c))) return rc;
-  const Grid& g = c->g;
-  long dimx = g.is3d ? (long)g.mk * (g.Nz + 1) : (long)g.mk;
-  c->npf = (dimx + 127) / 128 * 128;
-  c->gblocks = c->num_sms * 4;
-  const size_t tsz = c->precision == TDGL_MIXED ? sizeof(float) : sizeof(double);
-  const size_t full64 = (size_t)g.ncomp * c->npf * sizeof(double);
-  const size_t fullT = (size_t)g.ncomp * c->npf * tsz;
-  const size_t nb = (size_t)c->gblocks;
-  if ((rc = ctx_alloc(c, (void**)&c->Xn, c->L * sizeof(double)))) return rc;
-  if ((rc = ctx_alloc(c, (void**)&c->En, full64))) return rc;
-  if ((rc = ctx_alloc(c, (void**)&c->Ei, full64))) return rc;
-  if (c->precision == TDGL_MIXED) {
-    if ((rc = ctx_alloc(c, &c->XLe, fullT))) return rc;
-  } else {
-    c->XLe = c->Ei;
+  if (!c->gws_ready) {
+    const Grid& g = c->g;
+    long dimx = g.is3d ? (long)g.mk * (g.Nz + 1) : (long)g.mk;
+    c->npf = (dimx + 127) / 128 * 128;
+    const char* es = std::getenv("TDGL_STREAM_BLOCKS_PER_SM");
+    c->gblocks = c->num_sms * (es && std::atoi(es) > 0 ? std::atoi(es) : 8);
+    const size_t tsz = c->precision == TDGL_MIXED ? sizeof(float) : sizeof(double);
+    const size_t full64 = (size_t)g.ncomp * c->npf * sizeof(double);
+    const size_t fullT = (size_t)g.ncomp * c->npf * tsz;
+    const size_t nb = (size_t)c->gblocks;
+    if ((rc = ctx_alloc(c, (void**)&c->Xn, c->L * sizeof(double)))) return rc;
+    if ((rc = ctx_alloc(c, (void**)&c->En, full64))) return rc;
+    if ((rc = ctx_alloc(c, (void**)&c->Ei, full64))) return rc;
+    if (c->precision == TDGL_MIXED) {
+      if ((rc = ctx_alloc(c, &c->XLe, fullT))) return rc;
+    } else {
+      c->XLe = c->Ei;
+    }
+    if ((rc = ctx_alloc(c, &c->VE, fullT))) return rc;
+    if ((rc = ctx_alloc(c, (void**)&c->part_dots, sizeof(double) * (c->kmax + 1) * nb))) return rc;
+    if ((rc = ctx_alloc(c, (void**)&c->part_orth, sizeof(double) * nb))) return rc;
+    if ((rc = ctx_alloc(c, (void**)&c->part_nrhs, sizeof(double) * 3 * nb))) return rc;
+    if ((rc = ctx_alloc(c, (void**)&c->part_upd, sizeof(double) * nb))) return rc;
+    if ((rc = ctx_alloc(c, (void**)&c->kry, sizeof(double) * kry_len(c->kmax)))) return rc;
+    if ((rc = ctx_alloc(c, (void**)&c->gdev, sizeof(GDev)))) return rc;
+    TDGL_CUDA(cudaMallocHost((void**)&c->gdev_host, sizeof(GDev)));
+    const char* pe = std::getenv("TDGL_PROFILE");
+    c->gprof = pe && pe[0] && pe[0] != '0';
+    c->gws_ready = true;
   }
-  if ((rc = ctx_alloc(c, &c->VE, fullT))) return rc;
-  if ((rc = ctx_alloc(c, (void**)&c->part_dots, sizeof(double) * (c->kmax + 1) * nb))) return rc;
-  if ((rc = ctx_alloc(c, (void**)&c->part_orth, sizeof(double) * nb))) return rc;
-  if ((rc = ctx_alloc(c, (void**)&c->part_nrhs, sizeof(double) * 3 * nb))) return rc;
-  if ((rc = ctx_alloc(c, (void**)&c->part_upd, sizeof(double) * nb))) return rc;
-  if ((rc = ctx_alloc(c, (void**)&c->kry, sizeof(double) * kry_len(c->kmax)))) return rc;
-  if ((rc = ctx_alloc(c, (void**)&c->gdev, sizeof(GDev)))) return rc;
-  TDGL_CUDA(cudaMallocHost((void**)&c->gdev_host, sizeof(GDev)));
-  cudaError_t e = c->precision == TDGL_MIXED ? graph_build_f32(make_gargs<float>(c), &c->graph, &c->gexec)
-                                             : graph_build_f64(make_gargs<double>(c), &c->graph, &c->gexec);
+  if (v == 1 && (rc = ensure_arnoldi_ws(c))) return rc;
+  cudaError_t e;
+  if (c->precision == TDGL_MIXED) {
+    GArgs<float> A = make_gargs<float>(c);
+    A.fused = v;
+    e = graph_build_f32(A, &c->graph[v], &c->gexec[v]);
+  } else {
+    GArgs<double> A = make_gargs<double>(c);
+    A.fused = v;
+    e = graph_build_f64(A, &c->graph[v], &c->gexec[v]);
+  }
   if (e != cudaSuccess) {
-    if (c->graph) cudaGraphDestroy(c->graph);
-    c->graph = nullptr;
-    c->gexec = nullptr;
+    if (c->graph[v]) cudaGraphDestroy(c->graph[v]);
+    c->graph[v] = nullptr;
+    c->gexec[v] = nullptr;
     return fail(TDGL_ECUDA, std::string("building the stepper graph: ") + cudaGetErrorString(e));
   }
   return TDGL_OK;
@@ -568,7 +641,8 @@ static int graph_status(int gs) {
 static int run_graph(tdgl_ctx* c, double* x, double* t, double* dt_cur, int32_t max_steps, const tdgl_trap_opts* o,
                      const tdgl_field* f, tdgl_stats* st, tdgl_stream_t s) {
   int rc;
-  if ((rc = ensure_graph(c))) return rc;
+  const int v = o->jvp_mode == TDGL_JVP_ANALYTIC ? 1 : 0;
+  if ((rc = ensure_graph(c, v))) return rc;
   GDev& h = *c->gdev_host;
   std::memset(&h, 0, sizeof(GDev));
   h.t = *t;
@@ -594,6 +668,8 @@ static int run_graph(tdgl_ctx* c, double* x, double* t, double* dt_cur, int32_t 
   // hard limit on loop iterations: every step may be retried down to dt_min
   // (at most ~12 cuts of dt/10 in double range) with full Newton / Krylov loops
   h.watchdog_cap = (long long)(max_steps + 1) * 40 * (o->newton_max_iter + 2) * (c->kmax + 3) + 1000;
+  h.prof_on = c->gprof ? 1 : 0;
+  for (int k = 0; k < kKTypes; ++k) h.kt_start[k] = ~0ull;
   if (tdgl_stats* z = st) std::memset(z, 0, sizeof(*z));
   if (!(h.t < h.t_stop - 1e-14) || max_steps <= 0) {
     if (st) { st->t = h.t; st->dt_cur = h.dt_cur; }
@@ -601,12 +677,17 @@ static int run_graph(tdgl_ctx* c, double* x, double* t, double* dt_cur, int32_t 
   }
   TDGL_CUDA(cudaMemcpyAsync(c->Xn, x, c->L * sizeof(double), cudaMemcpyDeviceToDevice, s));
   TDGL_CUDA(cudaMemcpyAsync(c->gdev, &h, sizeof(GDev), cudaMemcpyHostToDevice, s));
-  TDGL_CUDA(cudaGraphLaunch(c->gexec, s));
+  if (c->ticket) TDGL_CUDA(cudaMemsetAsync(c->ticket, 0, sizeof(unsigned), s));
+  TDGL_CUDA(cudaGraphLaunch(c->gexec[v], s));
   TDGL_CUDA(cudaMemcpyAsync(&h, c->gdev, sizeof(GDev), cudaMemcpyDeviceToHost, s));
   TDGL_CUDA(cudaMemcpyAsync(x, c->Xn, c->L * sizeof(double), cudaMemcpyDeviceToDevice, s));
   TDGL_CUDA(cudaStreamSynchronize(s));
   *t = h.t;
   *dt_cur = h.dt_cur;
+  for (int k = 0; k < kKTypes; ++k) {
+    c->gk_total[k] += h.kt_total[k];
+    c->gk_count[k] += h.kt_count[k];
+  }
   if (st) {
     st->status = graph_status(h.status);
     st->steps = h.steps;
@@ -701,7 +782,37 @@ extern "C" int tdgl_euler_run(tdgl_ctx* c, double* x, double* t, double t_stop, 
   return TDGL_OK;
 }
 
+extern "C" int tdgl_arnoldi_probe(tdgl_ctx* c, int32_t ja, int32_t launches, tdgl_stream_t s) {
+  if (!c || launches < 0) return fail(TDGL_EINVAL, "invalid argument");
+  int rc;
+  if ((rc = ensure_graph(c, 1))) return rc;
+  if (ja < 0 || ja > c->kmax) return fail(TDGL_EINVAL, "ja must lie in [0, kmax]");
+  TDGL_CUDA(cudaMemcpyAsync(&c->gdev->ja, &ja, sizeof(int), cudaMemcpyHostToDevice, s));
+  cudaError_t e;
+  if (c->precision == TDGL_MIXED) {
+    GArgs<float> A = make_gargs<float>(c);
+    A.fused = 1;
+    A.standalone = 1;
+    e = arnoldi_probe_f32(A, launches, s);
+  } else {
+    GArgs<double> A = make_gargs<double>(c);
+    A.fused = 1;
+    A.standalone = 1;
+    e = arnoldi_probe_f64(A, launches, s);
+  }
+  if (e != cudaSuccess) return fail(TDGL_ECUDA, std::string("Arnoldi step launch: ") + cudaGetErrorString(e));
+  TDGL_CUDA(cudaStreamSynchronize(s));
+  return TDGL_OK;
+}
+
 extern "C" int tdgl_profile(tdgl_ctx* c, uint64_t* out, int64_t n, int32_t reset) {
+  if (c && c->gprof) {
+    for (int64_t k = 0; out && k < std::min<int64_t>(n, 2 * kKTypes); ++k)
+      out[k] = k < kKTypes ? c->gk_total[k] : (uint64_t)c->gk_count[k - kKTypes];
+    if (reset)
+      for (int k = 0; k < kKTypes; ++k) c->gk_total[k] = 0, c->gk_count[k] = 0;
+    return TDGL_OK;
+  }
   if (!c || !c->prof) return fail(TDGL_EINVAL, "phase timers are off (set TDGL_PROFILE=1 before creating the context)");
   int64_t m = std::min<int64_t>(n, kProfLen);
   if (out && m > 0) TDGL_CUDA(cudaMemcpy(out, c->prof, m * sizeof(uint64_t), cudaMemcpyDeviceToHost));

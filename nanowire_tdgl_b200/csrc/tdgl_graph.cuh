@@ -6,15 +6,17 @@
 // graph with nested conditional WHILE nodes:
 //
 //   STEP while { step_begin, prepare, predict, newton_rhs, newton_init,
-//     NEWTON while { KRYLOV while { stencil, dots, fin_dots, orth, fin_orth },
+//     NEWTON while { KRYLOV while { arn_orth, arn_apply },
 //                    newton_solve, update, newton_rhs, newton_check },
 //     accept, step_end }
 //
-// Grid kernels stream over the vectors and write per-block partial sums;
-// one-block kernels reduce them in a fixed order (repeatable sums), take every
-// control decision on the device and set the conditional handles.  No kernel
-// waits on another block, so nothing can spin; every loop also has a hard
-// iteration cap that aborts the launch with a status.
+// with KRYLOV while { stencil, dots, fin_dots, orth, fin_orth } for
+// finite-difference Jacobian products.  Grid kernels stream over the vectors
+// and write per-block partial sums; one-block kernels (or, in arn_apply, the
+// last block to finish) reduce them in a fixed order
+// (repeatable sums), take every control decision on the device and set the
+// conditional handles.  No kernel waits on another block, so nothing can spin;
+// every loop also has a hard iteration cap that aborts the launch with a status.
 //
 // Boundary handling: the pass that produces a vector that a stencil will read
 // (state, Newton iterate, linearisation copy, Arnoldi vector) also writes an
@@ -34,6 +36,8 @@ namespace tdgl {
 
 enum GStatus : int { GS_OK = 0, GS_NOCONV = 1, GS_DTMIN = 2, GS_KMAX = 3, GS_NONFINITE = 4, GS_CAP = 5 };
 
+constexpr int kKTypes = 16;   // slots of the per-kernel timers
+
 // Device control block of the graph executor.
 struct GDev {
   // inputs for one launch
@@ -48,7 +52,34 @@ struct GDev {
   // counters
   long long newton_iters, krylov_iters, krylov_sq, rhs_evals, jvp_evals, rejections;
   int max_krylov, krylov_last;
+  int ja;                          // basis vector the next Arnoldi step forms
+  // per-kernel timers (diagnostics, on when prof_on): first block start to
+  // last block end of each launch, summed per kernel type
+  int prof_on;
+  unsigned long long kt_start[kKTypes], kt_end[kKTypes], kt_total[kKTypes];
+  long long kt_count[kKTypes];
 };
+
+enum KType : int { KT_PREPARE = 0, KT_PREDICT, KT_NRHS, KT_STENCIL, KT_DOTS, KT_ORTH, KT_UPDATE, KT_ACCEPT, KT_ARN_APPLY, KT_ARN_ORTH, KT_ARN_DOTS };
+
+__device__ __forceinline__ void kt_begin(GDev* d, int k) {
+  if (d->prof_on && threadIdx.x == 0) atomicMin(&d->kt_start[k], global_ns());
+}
+__device__ __forceinline__ void kt_end(GDev* d, int k) {
+  if (d->prof_on) {
+    __syncthreads();
+    if (threadIdx.x == 0) atomicMax(&d->kt_end[k], global_ns());
+  }
+}
+// Fold the last launch of kernel type k into its total (thread 0 of a one-block kernel).
+__device__ __forceinline__ void kt_fold(GDev* d, int k) {
+  if (d->prof_on && d->kt_end[k] > 0) {
+    d->kt_total[k] += d->kt_end[k] - d->kt_start[k];
+    d->kt_count[k] += 1;
+    d->kt_start[k] = ~0ull;
+    d->kt_end[k] = 0;
+  }
+}
 
 template <typename T>
 struct GArgs {
@@ -73,6 +104,21 @@ struct GArgs {
   long npf;            // full-grid component stride
   int kmax, nblk;
   cudaGraphConditionalHandle h_step, h_newton, h_krylov;
+  // two-kernel Arnoldi form (analytic Jacobian products): unnormalised basis U_0..U_kmax
+  // and A U_j (ping-pong) on the full grid -- raw values at interior nodes, the
+  // boundary procedure's face values (no field offsets) at face nodes, zero at edges
+  int fused;
+  T* UB;               // (kmax + 1) vectors of vs entries
+  T* Zb[2];
+  long vs;             // ncomp * npf
+  double* part_arn;    // [(kmax + 2) x nblk_arn]
+  unsigned* ticket;    // arrival counter of kg_arn_dots (the last block reduces)
+  int nblk_arn;        // blocks of kg_arn_dots
+  int nblk_orth;       // blocks of kg_arn_orth (<= nblk: its partials go to part_orth)
+  int arn_gx, arn_gy;  // grid of kg_arn_apply: (ceil(nx / 32), ceil(ny / 8), nz), 32 x 8 nodes a block
+  const uint8_t* imask;   // full grid: 1 at interior nodes
+  double cxu, cyu, czu;   // uniform kappa^2 / h^2 (node_coef's values without a per-node kappa)
+  int standalone;      // diagnostic launch outside the graph: no bookkeeping, no conditionals
 };
 
 template <typename T> __host__ __device__ __forceinline__ double* kry_sj(const GArgs<T>& A) { return A.kry; }
@@ -124,7 +170,9 @@ __device__ __forceinline__ long full_index(const Grid& g, int i, int j, int k) {
 // Write node (i, j, k)'s effective values and the face values copied from it.
 // v: raw values (psi re, psi im, phi x, phi y, phi z); c*: face offsets of the
 // applied field (zero for tangent vectors).
-template <typename T, bool D3>
+// RAW_OWN: the node itself keeps its raw values (dead links included); only
+// the face copies get the boundary procedure.
+template <typename T, bool D3, bool RAW_OWN = false>
 __device__ __forceinline__ void write_eff(const Grid& g, T* E, long npf, int i, int j, int k, const double* v,
                                           double czxy, double cyzx, double cxyz) {
   const long m = full_index(g, i, j, k);
@@ -134,9 +182,15 @@ __device__ __forceinline__ void write_eff(const Grid& g, T* E, long npf, int i, 
   const double tz = (D3 && k == g.Nz - 1) ? 0.0 : (D3 ? v[4] : 0.0);
   E[m] = (T)v[0];
   E[npf + m] = (T)v[1];
-  E[2 * npf + m] = (lf & LF_HX) ? T(0) : (T)tx;
-  E[3 * npf + m] = (lf & LF_HY) ? T(0) : (T)ty;
-  if (D3) E[4 * npf + m] = (lf & LF_HZ) ? T(0) : (T)tz;
+  if (RAW_OWN) {
+    E[2 * npf + m] = (T)v[2];
+    E[3 * npf + m] = (T)v[3];
+    if (D3) E[4 * npf + m] = (T)v[4];
+  } else {
+    E[2 * npf + m] = (lf & LF_HX) ? T(0) : (T)tx;
+    E[3 * npf + m] = (lf & LF_HY) ? T(0) : (T)ty;
+    if (D3) E[4 * npf + m] = (lf & LF_HZ) ? T(0) : (T)tz;
+  }
   auto ghost = [&](long mg, double fx, double fy, double fz) {
     const uint8_t lg = g.lflags ? g.lflags[mg] : 0;
     E[mg] = (T)v[0];
@@ -229,6 +283,7 @@ __device__ __forceinline__ void abort_all(const GArgs<T>& A, int status) {
 template <typename T>
 __device__ __forceinline__ bool krylov_start(const GArgs<T>& A, GDev* d) {
   d->j = 0;
+  d->ja = 0;
   d->rho = d->rho0;
   kry_gv(A)[0] = d->rho0;
   kry_sj(A)[0] = d->rho0 > 0.0 ? 1.0 / d->rho0 : 0.0;
@@ -245,6 +300,7 @@ template <typename T, bool D3>
 __global__ void __launch_bounds__(kThreads) kg_prepare(GArgs<T> A) {
   const GDev* d = A.dev;
   if (!gdev_ok(d)) return;
+  kt_begin(A.dev, KT_PREPARE);
   const Grid& g = A.g;
   const double czxy = d->czxy, cyzx = d->cyzx, cxyz = d->cxyz;
   for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < g.n; n += gridDim.x * blockDim.x) {
@@ -255,6 +311,7 @@ __global__ void __launch_bounds__(kThreads) kg_prepare(GArgs<T> A) {
     for (int c = 0; c < (D3 ? 5 : 4); ++c) v[c] = A.Xn[(long)c * g.npad + n];
     write_eff<double, D3>(g, A.En, A.npf, i, j, k, v, czxy, cyzx, cxyz);
   }
+  kt_end(A.dev, KT_PREPARE);
 }
 
 // Predictor: f = rhs(Xn); Xi = Xn + dt f; G = Xn + dt/2 f (integrators.py:156-158);
@@ -263,6 +320,7 @@ template <typename T, bool D3>
 __global__ void __launch_bounds__(kThreads) kg_predict(GArgs<T> A) {
   const GDev* d = A.dev;
   if (!gdev_ok(d)) return;
+  kt_begin(A.dev, KT_PREDICT);
   const Grid& g = A.g;
   const double dt = d->dta, czxy = d->czxy, cyzx = d->cyzx, cxyz = d->cxyz;
   for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < g.n; n += gridDim.x * blockDim.x) {
@@ -285,6 +343,7 @@ __global__ void __launch_bounds__(kThreads) kg_predict(GArgs<T> A) {
     write_eff<double, D3>(g, A.Ei, A.npf, i, j, k, xi, czxy, cyzx, cxyz);
     if ((void*)A.XLe != (void*)A.Ei) write_eff<T, D3>(g, A.XLe, A.npf, i, j, k, xi, czxy, cyzx, cxyz);
   }
+  kt_end(A.dev, KT_PREDICT);
 }
 
 // Newton residual: f = rhs(Xi) into F; g = Xi - dt/2 f - G; r0 = -g into the
@@ -293,6 +352,7 @@ template <typename T, bool D3>
 __global__ void __launch_bounds__(kThreads) kg_newton_rhs(GArgs<T> A) {
   const GDev* d = A.dev;
   if (!gdev_ok(d) || d->newton_failed) return;
+  kt_begin(A.dev, KT_NRHS);
   const Grid& g = A.g;
   const double dt = d->dta;
   double acc[3] = {0.0, 0.0, 0.0};
@@ -312,7 +372,7 @@ __global__ void __launch_bounds__(kThreads) kg_newton_rhs(GArgs<T> A) {
       A.F[e] = o[c];
       gv[c] = xv - (dt / 2.0) * o[c] - A.G[e];
       T rt = (T)(-gv[c]);
-      A.V[e] = rt;
+      if (!A.fused) A.V[e] = rt;
       r[c] = (double)rt;
       acc[0] += r[c] * r[c];
       acc[1] += xv * xv;
@@ -321,10 +381,12 @@ __global__ void __launch_bounds__(kThreads) kg_newton_rhs(GArgs<T> A) {
 #pragma unroll
     for (int c = 2; c < (D3 ? 5 : 4); ++c) m = fmax(m, gfinite(fabs(gv[c])));
     acc[2] = fmax(acc[2], m);
-    write_eff<T, D3>(g, A.VE, A.npf, i, j, k, r, 0.0, 0.0, 0.0);
+    if (A.fused) write_eff<T, D3, true>(g, A.UB, A.npf, i, j, k, r, 0.0, 0.0, 0.0);
+    else write_eff<T, D3>(g, A.VE, A.npf, i, j, k, r, 0.0, 0.0, 0.0);
   }
   const bool mx[3] = {false, false, true};
   block_partials<3>(acc, mx, A.part_nrhs, A.nblk);
+  kt_end(A.dev, KT_NRHS);
 }
 
 // Arnoldi stencil: W = A v_j, v_j = s_j v~_j (basis slot j-1, effective copy VE).
@@ -332,6 +394,7 @@ template <typename T, bool D3>
 __global__ void __launch_bounds__(kThreads) kg_stencil(GArgs<T> A) {
   const GDev* d = A.dev;
   if (!gdev_ok(d)) return;
+  kt_begin(A.dev, KT_STENCIL);
   const Grid& g = A.g;
   const int jc = d->j + 1;
   const double sj = kry_sj(A)[jc - 1];
@@ -365,6 +428,7 @@ __global__ void __launch_bounds__(kThreads) kg_stencil(GArgs<T> A) {
 #pragma unroll
     for (int c = 0; c < (D3 ? 5 : 4); ++c) A.W[(long)c * g.npad + n] = (T)w[c];
   }
+  kt_end(A.dev, KT_STENCIL);
 }
 
 template <typename T> struct GGroup { static constexpr int JB = 8; };
@@ -392,6 +456,7 @@ template <typename T>
 __global__ void __launch_bounds__(kThreads) kg_dots(GArgs<T> A) {
   const GDev* d = A.dev;
   if (!gdev_ok(d)) return;
+  kt_begin(A.dev, KT_DOTS);
   constexpr int JB = GGroup<T>::JB;
   __shared__ double red[kWarps][JB];
   const int jc = d->j + 1;
@@ -423,6 +488,7 @@ __global__ void __launch_bounds__(kThreads) kg_dots(GArgs<T> A) {
     }
     __syncthreads();
   }
+  kt_end(A.dev, KT_DOTS);
 }
 
 // Orthogonalisation: v~_{j+1} = W - sum_{i<j} gam_i v~_i (raw, slot j) and its
@@ -431,6 +497,7 @@ template <typename T, bool D3>
 __global__ void __launch_bounds__(kThreads) kg_orth(GArgs<T> A) {
   const GDev* d = A.dev;
   if (!gdev_ok(d)) return;
+  kt_begin(A.dev, KT_ORTH);
   constexpr int JB = GGroup<T>::JB;
   constexpr int NC = D3 ? 5 : 4;
   const Grid& g = A.g;
@@ -480,6 +547,7 @@ __global__ void __launch_bounds__(kThreads) kg_orth(GArgs<T> A) {
   }
   const bool mx[1] = {false};
   block_partials<1>(acc, mx, A.part_orth, A.nblk);
+  kt_end(A.dev, KT_ORTH);
 }
 
 // Newton update: x += sum_i cj_i v~_i (raw FP64), effective copies of the new
@@ -488,6 +556,7 @@ template <typename T, bool D3>
 __global__ void __launch_bounds__(kThreads) kg_update(GArgs<T> A) {
   const GDev* d = A.dev;
   if (!gdev_ok(d) || d->newton_failed) return;
+  kt_begin(A.dev, KT_UPDATE);
   constexpr int JB = GGroup<T>::JB;
   constexpr int NC = D3 ? 5 : 4;
   const Grid& g = A.g;
@@ -495,6 +564,49 @@ __global__ void __launch_bounds__(kThreads) kg_update(GArgs<T> A) {
   const double* cj = kry_cj(A);
   const double czxy = d->czxy, cyzx = d->cyzx, cxyz = d->cxyz;
   double acc[1] = {0.0};
+  if (A.fused) {
+    // basis on the full grid: one node per thread
+    for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < g.n; n += gridDim.x * blockDim.x) {
+      int i, j, k;
+      node_ijk(g, n, i, j, k);
+      const long m = full_index(g, i, j, k);
+      double s[NC], v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+      for (int c = 0; c < NC; ++c) s[c] = 0.0;
+      int i0 = 0;
+      for (; i0 + 4 <= nk; i0 += 4) {
+        const T* U = A.UB + (long)i0 * A.vs + m;
+        const double c0 = cj[i0], c1 = cj[i0 + 1], c2 = cj[i0 + 2], c3 = cj[i0 + 3];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+          const long e = (long)c * A.npf;
+          s[c] += c0 * (double)U[e] + c1 * (double)U[A.vs + e] + c2 * (double)U[2 * A.vs + e] +
+                  c3 * (double)U[3 * A.vs + e];
+        }
+      }
+      for (; i0 < nk; ++i0) {
+        const T* U = A.UB + (long)i0 * A.vs + m;
+#pragma unroll
+        for (int c = 0; c < NC; ++c) s[c] += cj[i0] * (double)U[(long)c * A.npf];
+      }
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        const long e = (long)c * g.npad + n;
+        v[c] = A.Xi[e] + s[c];
+        A.Xi[e] = v[c];
+      }
+      double mm = gfinite(hypot(s[0], s[1]));
+#pragma unroll
+      for (int c = 2; c < NC; ++c) mm = fmax(mm, gfinite(fabs(s[c])));
+      acc[0] = fmax(acc[0], mm);
+      write_eff<double, D3>(g, A.Ei, A.npf, i, j, k, v, czxy, cyzx, cxyz);
+      if ((void*)A.XLe != (void*)A.Ei) write_eff<T, D3>(g, A.XLe, A.npf, i, j, k, v, czxy, cyzx, cxyz);
+    }
+    const bool mx[1] = {true};
+    block_partials<1>(acc, mx, A.part_upd, A.nblk);
+    kt_end(A.dev, KT_UPDATE);
+    return;
+  }
   const long nq = g.npad / 4;
   for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < nq; q += (long)gridDim.x * blockDim.x) {
     const long base = 4 * q;
@@ -539,6 +651,7 @@ __global__ void __launch_bounds__(kThreads) kg_update(GArgs<T> A) {
   }
   const bool mx[1] = {true};
   block_partials<1>(acc, mx, A.part_upd, A.nblk);
+  kt_end(A.dev, KT_UPDATE);
 }
 
 // Accepted step: Xn = Xi.
@@ -546,9 +659,305 @@ template <typename T>
 __global__ void __launch_bounds__(kThreads) kg_accept(GArgs<T> A) {
   const GDev* d = A.dev;
   if (!gdev_ok(d) || !d->accepted) return;
+  kt_begin(A.dev, KT_ACCEPT);
   const long nq = A.L / 2;
   for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < nq; q += (long)gridDim.x * blockDim.x)
     reinterpret_cast<double2*>(A.Xn)[q] = reinterpret_cast<const double2*>(A.Xi)[q];
+  kt_end(A.dev, KT_ACCEPT);
+}
+
+// ---------------------------------------------------------------------------
+// Two-kernel Arnoldi step (analytic Jacobian products)
+// ---------------------------------------------------------------------------
+//
+// Step ja of a Krylov solve runs
+//   kg_arn_orth   U_ja = Z_{ja-1} - sum_{i<ja} gam_i U_i   (nothing for ja = 0: U_0 = r0,
+//                 written by the Newton residual)
+//   kg_arn_apply  Z_ja = U_ja - dt/2 J(x) U_ja  (A U_ja; the tangent-linear product is
+//                 linear)
+//   kg_arn_dots   <Z_ja, U_i> (i <= ja) over the interior entries (||U_ja||^2 comes
+//                 with the orthogonalisation).
+// The basis stays unnormalised (v_i = s_i U_i, s_i = 1 / ||U_i||): with
+// gam_i = s_i^2 <Z_{ja-1}, U_i>, U_ja is the classical Gram-Schmidt remainder of
+// A v_{ja-1} divided by s_{ja-1}.  The last block of kg_arn_dots adds the
+// partials in a fixed order, completes Hessenberg column ja-1 (norm, Givens
+// rotation, residual estimate and the stop test of tgcr.py:125, 141-142) and,
+// when the iteration goes on, stores column ja and the next coefficients.  A
+// solve of m iterations takes m + 1 steps; the last product is not used.
+//
+// The vectors live on the full grid with their face values, and the boundary
+// procedure is linear for directions, so kg_arn_orth combines every entry
+// (faces, edges, padding) without looking at positions.  kg_arn_apply reads
+// the raw values and zeroes the dead links of the stencil's neighbours (normal
+// links on plane N-1, hole links) on the fly.
+
+// Column bookkeeping of launch ja (thread 0 of the last block).  S[i] = <Z_ja, U_i>, S[ja+1] = ||U_ja||^2.
+template <typename T>
+__device__ void arn_finish(const GArgs<T>& A, GDev* d, int ja, const double* S) {
+  if (++d->watchdog > d->watchdog_cap) { abort_all(A, GS_CAP); return; }
+  double* sj = kry_sj(A);
+  double* gam = kry_gam(A);
+  for (int i = 0; i <= ja + 1; ++i)
+    if (!isfinite(S[i])) { abort_all(A, GS_NONFINITE); return; }
+  if (ja > 0) {
+    const int jc = ja;                                   // columns complete after this launch
+    double* gv = kry_gv(A);
+    double* cs = kry_cs(A);
+    double* sn = kry_sn(A);
+    double* col = kry_H(A) + (long)(jc - 1) * (A.kmax + 1);
+    const double un = sqrt(S[ja + 1]);
+    const double hn = un * sj[jc - 1];                   // h_{jc, jc-1} = ||A v - sum h v||
+    sj[jc] = un > 0.0 ? 1.0 / un : 0.0;
+    d->jvp_evals += 1;
+    col[jc] = hn;
+    for (int i = 0; i + 1 < jc; ++i) {
+      double a = col[i], b = col[i + 1];
+      col[i] = cs[i] * a + sn[i] * b;
+      col[i + 1] = -sn[i] * a + cs[i] * b;
+    }
+    double a = col[jc - 1], b = col[jc];
+    double r = hypot(a, b);
+    double c = r > 0.0 ? a / r : 1.0, sv = r > 0.0 ? b / r : 0.0;
+    cs[jc - 1] = c;
+    sn[jc - 1] = sv;
+    col[jc - 1] = r;
+    col[jc] = 0.0;
+    gv[jc] = -sv * gv[jc - 1];
+    gv[jc - 1] = c * gv[jc - 1];
+    d->rho = fabs(gv[jc]);
+    d->j = jc;
+    bool cont = hn > 0.0 && d->rho / d->rho0 > d->tol_gcr && jc < d->krylov_max_iter;
+    if (cont && jc + 1 > A.kmax) { abort_all(A, GS_KMAX); return; }
+    if (!cont) { cudaGraphSetConditional(A.h_krylov, 0); return; }
+  }
+  double* colj = kry_H(A) + (long)ja * (A.kmax + 1);
+  for (int i = 0; i <= ja; ++i) {
+    colj[i] = sj[ja] * sj[i] * S[i];
+    gam[i] = sj[i] * sj[i] * S[i];
+  }
+  d->ja = ja + 1;
+  cudaGraphSetConditional(A.h_krylov, 1);
+}
+
+// Per-thread asynchronous copies global -> shared (no alignment beyond the
+// element size); each thread later reads only the slots it filled itself.
+template <typename T>
+__device__ __forceinline__ void cp_async_elem(T* dst, const T* src) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+  if (sizeof(T) == 4) asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(src) : "memory");
+  else asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+
+// Neighbourhood of a direction vector stored raw at interior nodes: the
+// stencil sees the normal link zeroed on plane N-1 of its axis and hole links
+// zeroed.  Face entries already hold the boundary procedure's values, which
+// satisfy the same rules.
+template <typename T>
+struct NbM {
+  const T* E; long npf; long m; int mj, mk; int i, j, k; const Grid* g; const uint8_t* lflags;
+  __device__ __forceinline__ void psi(int di, int dj, int dk, T& re, T& im) const {
+    long e = m + di + (long)dj * mj + (long)dk * mk;
+    re = E[e];
+    im = E[npf + e];
+  }
+  // branch-free: both loads are issued before the select
+  __device__ __forceinline__ T phi(int a, int di, int dj, int dk) const {
+    const long e = m + di + (long)dj * mj + (long)dk * mk;
+    const T v = E[(2 + a) * npf + e];
+    const unsigned lf = lflags ? (unsigned)lflags[e] : 0u;
+    const bool dead = (a == 0 && i + di == g->Nx - 1) || (a == 1 && j + dj == g->Ny - 1) ||
+                      (a == 2 && k + dk == g->Nz - 1) || ((lf >> a) & 1u);
+    return dead ? T(0) : v;
+  }
+};
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 5 : 3) kg_arn_orth(GArgs<T> A) {
+  GDev* d = A.dev;
+  if (!gdev_ok(d)) return;
+  const int ja = d->ja;
+  if (ja == 0) return;
+  kt_begin(d, KT_ARN_ORTH);
+  extern __shared__ double gsm[];              // gam_0 .. gam_{ja-1}
+  for (int t = threadIdx.x; t < ja; t += blockDim.x) gsm[t] = kry_gam(A)[t];
+  __syncthreads();
+  const T* Zin = A.Zb[(ja + 1) & 1];
+  T* Uj = A.UB + (long)ja * A.vs;
+  const long vs = A.vs, npf = A.npf, nq = vs / 4;
+  const long stride = (long)gridDim.x * blockDim.x;
+  long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  long mo = (4 * q) % npf;                     // offset within the component (interior mask)
+  double nrm = 0.0;
+  for (; q < nq; q += stride) {
+    const long e = 4 * q;
+    const V4<T> z = ld4(Zin + e);
+    double v[4] = {(double)z.a, (double)z.b, (double)z.c, (double)z.d};
+    const T* U = A.UB + e;
+    int i = 0;
+    for (; i + 4 <= ja; i += 4) {
+      const V4<T> a0 = ld4(U + (long)i * vs), a1 = ld4(U + (long)(i + 1) * vs);
+      const V4<T> a2 = ld4(U + (long)(i + 2) * vs), a3 = ld4(U + (long)(i + 3) * vs);
+      const double g0 = gsm[i], g1 = gsm[i + 1], g2 = gsm[i + 2], g3 = gsm[i + 3];
+      v[0] -= g0 * (double)a0.a + g1 * (double)a1.a + g2 * (double)a2.a + g3 * (double)a3.a;
+      v[1] -= g0 * (double)a0.b + g1 * (double)a1.b + g2 * (double)a2.b + g3 * (double)a3.b;
+      v[2] -= g0 * (double)a0.c + g1 * (double)a1.c + g2 * (double)a2.c + g3 * (double)a3.c;
+      v[3] -= g0 * (double)a0.d + g1 * (double)a1.d + g2 * (double)a2.d + g3 * (double)a3.d;
+    }
+    for (; i < ja; ++i) {
+      const V4<T> a = ld4(U + (long)i * vs);
+      const double g = gsm[i];
+      v[0] -= g * (double)a.a; v[1] -= g * (double)a.b; v[2] -= g * (double)a.c; v[3] -= g * (double)a.d;
+    }
+#pragma unroll
+    for (int t = 0; t < 4; ++t) v[t] = (double)(T)v[t];
+    st4(Uj + e, v);
+    const uchar4 mk = *reinterpret_cast<const uchar4*>(A.imask + mo);
+    nrm += (mk.x ? v[0] * v[0] : 0.0) + (mk.y ? v[1] * v[1] : 0.0) + (mk.z ? v[2] * v[2] : 0.0) +
+           (mk.w ? v[3] * v[3] : 0.0);
+    mo += 4 * stride;
+    while (mo >= npf) mo -= npf;
+  }
+  double acc[1] = {nrm};
+  const bool mx[1] = {false};
+  block_partials<1>(acc, mx, A.part_orth, A.nblk_orth);
+  kt_end(d, KT_ARN_ORTH);
+}
+
+template <typename T, bool D3>
+__global__ void __launch_bounds__(kThreads, 3) kg_arn_apply(GArgs<T> A) {
+  GDev* d = A.dev;
+  if (!gdev_ok(d)) return;
+  kt_begin(d, KT_ARN_APPLY);
+  constexpr int NC = D3 ? 5 : 4;
+  const Grid& g = A.g;
+  const int ja = d->ja;
+  const long npf = A.npf;
+  const T* Uj = A.UB + (long)ja * A.vs;
+  T* Zout = A.Zb[ja & 1];
+  const double dth = d->dta / 2.0;
+  const int i = 1 + blockIdx.x * 32 + (threadIdx.x & 31), j = 1 + blockIdx.y * 8 + (threadIdx.x >> 5);
+  const int k = D3 ? 1 + (int)blockIdx.z : 0;
+  if (i <= g.nx && j <= g.ny) {
+    const int n = dix(g, i, j, k);
+    const long m = full_index(g, i, j, k);
+    const uint8_t nf = g.nflags[n];
+    NodeCoef<T> nc;
+    if (g.kappa_per_node) nc = node_coef<T>(g, n, nf);
+    else {
+      nc.cx = (T)A.cxu; nc.cy = (T)A.cyu; nc.cz = (T)A.czu;
+      nc.material = g.has_material != 0;
+      if (!nc.material) nc.sc = T(1);
+      else if (nf & NF_SCFRAC) nc.sc = (T)g.scint[n];
+      else nc.sc = (nf & NF_SC0) ? T(0) : T(1);
+    }
+    NbE<T, T> X{A.XLe, npf, m, g.mj, g.mk};
+    NbM<T> P{Uj, npf, m, g.mj, g.mk, i, j, k, &g, g.lflags};
+    T o[5];
+    jvp_body<T, D3>(g, X, P, nc, nf, o);
+    double z[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int c = 0; c < NC; ++c) z[c] = (double)Uj[c * npf + m] - dth * (double)o[c];
+    write_eff<T, D3, true>(g, Zout, npf, i, j, k, z, 0.0, 0.0, 0.0);
+  }
+  kt_end(d, KT_ARN_APPLY);
+}
+
+// Projections <Z_ja, U_i> (i <= ja) over the interior entries (imask), in
+// passes over groups of GGroup<T>::JB vectors whose loads are all in flight
+// together.  A thread's few products per vector are summed in T (the vectors'
+// precision), warps and blocks sum in double; the last block to finish adds
+// the block partials and the orthogonalisation's ||U_ja||^2 partials in a
+// fixed order and does the column bookkeeping.
+template <typename T>
+__global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 5 : 4) kg_arn_dots(GArgs<T> A) {
+  GDev* d = A.dev;
+  if (!gdev_ok(d)) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) abort_all(A, d->status);
+    return;
+  }
+  kt_begin(d, KT_ARN_DOTS);
+  __shared__ bool last_block;
+  extern __shared__ double red[];              // [kWarps][ja + 2]
+  const int ja = d->ja;
+  const int nd = ja + 2;
+  const T* Z = A.Zb[ja & 1];
+  const long vs = A.vs, npf = A.npf, nq = vs / 4;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int t = threadIdx.x; t < kWarps * nd; t += blockDim.x) red[t] = 0.0;
+  __syncthreads();
+  constexpr int DG = GGroup<T>::JB;            // vectors per pass: their loads are all in flight at once
+  const long stride = (long)gridDim.x * blockDim.x;
+  const long q0 = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const long mo0 = (4 * q0) % npf;
+  for (int i0 = 0; i0 <= ja; i0 += DG) {
+    T acc[DG];
+#pragma unroll
+    for (int t = 0; t < DG; ++t) acc[t] = T(0);
+    long mo = mo0;
+    for (long q = q0; q < nq; q += stride) {
+      const long e = 4 * q;
+      V4<T> z = ld4(Z + e);
+      V4<T> a[DG];
+#pragma unroll
+      for (int t = 0; t < DG; ++t) a[t] = (i0 + t <= ja) ? ld4(A.UB + (long)(i0 + t) * vs + e) : V4<T>{0, 0, 0, 0};
+      const uchar4 mk = *reinterpret_cast<const uchar4*>(A.imask + mo);
+      if (!mk.x) z.a = T(0);
+      if (!mk.y) z.b = T(0);
+      if (!mk.z) z.c = T(0);
+      if (!mk.w) z.d = T(0);
+#pragma unroll
+      for (int t = 0; t < DG; ++t) acc[t] += z.a * a[t].a + z.b * a[t].b + z.c * a[t].c + z.d * a[t].d;
+      mo += 4 * stride;
+      while (mo >= npf) mo -= npf;
+    }
+#pragma unroll
+    for (int t = 0; t < DG; ++t) {
+      const double v = warp_sum((double)acc[t]);
+      if (lane == 0 && i0 + t <= ja) red[warp * nd + i0 + t] = v;
+    }
+  }
+  __syncthreads();
+  for (int s = threadIdx.x; s <= ja; s += blockDim.x) {
+    double a = 0.0;
+    for (int w = 0; w < kWarps; ++w) a += red[w * nd + s];
+    A.part_arn[(long)s * A.nblk_arn + blockIdx.x] = a;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last_block = atomicAdd(A.ticket, 1u) == (unsigned)A.nblk_arn - 1;
+  __syncthreads();
+  if (!last_block) return;
+  __threadfence();
+  // fixed-order fold of the partials (L2 reads: other blocks wrote them)
+  double* S = red;
+  for (int s = warp; s < nd; s += kWarps) {
+    double a = 0.0;
+    if (s <= ja) {
+      for (int bb = lane; bb < A.nblk_arn; bb += 32) a += __ldcg(A.part_arn + (long)s * A.nblk_arn + bb);
+    } else if (ja > 0) {       // ||U_ja||^2 from the orthogonalisation's partials
+      for (int bb = lane; bb < A.nblk_orth; bb += 32) a += __ldcg(A.part_orth + bb);
+    }
+    a = warp_sum(a);
+    if (lane == 0) S[s] = a;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    *A.ticket = 0u;
+    if (A.standalone) return;
+    if (d->status != GS_OK) { abort_all(A, d->status); return; }
+    kt_fold(d, KT_ARN_ORTH);
+    kt_fold(d, KT_ARN_APPLY);
+    arn_finish(A, d, ja, S);
+    if (d->prof_on) {
+      d->kt_total[KT_ARN_DOTS] += global_ns() - d->kt_start[KT_ARN_DOTS];
+      d->kt_count[KT_ARN_DOTS] += 1;
+      d->kt_start[KT_ARN_DOTS] = ~0ull;
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -593,6 +1002,9 @@ __global__ void kg_newton_init(GArgs<T> A) {
   reduce_parts(A.part_nrhs, A.nblk, 2, false, s);
   reduce_parts(A.part_nrhs + 2L * A.nblk, A.nblk, 1, true, s + 2);
   if (threadIdx.x != 0) return;
+  kt_fold(d, KT_PREPARE);
+  kt_fold(d, KT_PREDICT);
+  kt_fold(d, KT_NRHS);
   d->rhs_evals += 1;
   d->rho0 = sqrt(s[0]);
   d->xnorm = sqrt(s[1]);
@@ -611,6 +1023,10 @@ __global__ void kg_fin_dots(GArgs<T> A) {
   if (d->status != GS_OK) return;
   const int jc = d->j + 1;
   reduce_parts(A.part_dots, A.nblk, jc, false, sh);
+  if (threadIdx.x == 0) {
+    kt_fold(d, KT_STENCIL);
+    kt_fold(d, KT_DOTS);
+  }
   double* sj = kry_sj(A);
   double* gam = kry_gam(A);
   double* col = kry_H(A) + (long)(jc - 1) * (A.kmax + 1);
@@ -631,6 +1047,7 @@ __global__ void kg_fin_orth(GArgs<T> A) {
   reduce_parts(A.part_orth, A.nblk, 1, false, s);
   if (threadIdx.x != 0) return;
   if (++d->watchdog > d->watchdog_cap) { abort_all(A, GS_CAP); return; }
+  kt_fold(d, KT_ORTH);
   const int jc = d->j + 1;
   d->jvp_evals += 1;
   double hn = sqrt(s[0]);
@@ -706,6 +1123,8 @@ __global__ void kg_newton_check(GArgs<T> A) {
   reduce_parts(A.part_upd, A.nblk, 1, true, s + 3);
   if (threadIdx.x != 0) return;
   if (++d->watchdog > d->watchdog_cap) { abort_all(A, GS_CAP); return; }
+  kt_fold(d, KT_UPDATE);
+  kt_fold(d, KT_NRHS);
   d->rhs_evals += 1;
   d->newton_iters += 1;
   d->rho0 = sqrt(s[0]);
@@ -734,6 +1153,7 @@ template <typename T>
 __global__ void kg_step_end(GArgs<T> A) {
   if (threadIdx.x != 0) return;
   GDev* d = A.dev;
+  kt_fold(d, KT_ACCEPT);
   if (d->status == GS_OK) {
     if (d->accepted) {
       d->t += d->dta;

@@ -1,5 +1,8 @@
 // Construction of the trapezoidal-stepper graph (see tdgl_graph.cuh): kernel
-// nodes chained linearly inside three nested conditional WHILE bodies.
+// nodes chained linearly inside three nested conditional WHILE bodies.  The
+// Krylov body is the three-kernel Arnoldi step for analytic Jacobian products, or
+// stencil / projection / orthogonalisation kernels with one-block reductions
+// for finite-difference products.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -12,10 +15,10 @@ struct Chain {
   cudaGraph_t g;
   cudaGraphNode_t last = nullptr;
   template <class Args>
-  cudaError_t kernel(const void* fn, int grid, int block, size_t smem, Args& args) {
+  cudaError_t kernel(const void* fn, dim3 grid, int block, size_t smem, Args& args) {
     cudaKernelNodeParams p{};
     p.func = const_cast<void*>(fn);
-    p.gridDim = dim3(grid);
+    p.gridDim = grid;
     p.blockDim = dim3(block);
     p.sharedMemBytes = (unsigned)smem;
     void* a[] = {&args};
@@ -76,11 +79,22 @@ cudaError_t build_trap_graph(GArgs<T> A, cudaGraph_t* out_graph, cudaGraphExec_t
   TDGL_GCK(cn.kernel((const void*)kg_newton_rhs<T, D3>, nb, kThreads, 0, A));
   TDGL_GCK(cn.kernel((const void*)kg_newton_check<T>, 1, kThreads, 0, A));
   Chain ck{krylov_body};
-  TDGL_GCK(ck.kernel((const void*)kg_stencil<T, D3>, nb, kThreads, 0, A));
-  TDGL_GCK(ck.kernel((const void*)kg_dots<T>, nb, kThreads, 0, A));
-  TDGL_GCK(ck.kernel((const void*)kg_fin_dots<T>, 1, kThreads, fin_smem, A));
-  TDGL_GCK(ck.kernel((const void*)kg_orth<T, D3>, nb, kThreads, 0, A));
-  TDGL_GCK(ck.kernel((const void*)kg_fin_orth<T>, 1, kThreads, 0, A));
+  if (A.fused) {
+    const size_t smo = (size_t)(A.kmax + 1) * sizeof(double);
+    const size_t smd = (size_t)kWarps * (A.kmax + 2) * sizeof(double);
+    TDGL_GCK(cudaFuncSetAttribute((const void*)kg_arn_orth<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smo));
+    TDGL_GCK(cudaFuncSetAttribute((const void*)kg_arn_dots<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smd));
+    TDGL_GCK(ck.kernel((const void*)kg_arn_orth<T>, A.nblk_orth, kThreads, smo, A));
+    TDGL_GCK(ck.kernel((const void*)kg_arn_apply<T, D3>, dim3(A.arn_gx, A.arn_gy, D3 ? A.g.nz : 1), kThreads, 0,
+                       A));
+    TDGL_GCK(ck.kernel((const void*)kg_arn_dots<T>, A.nblk_arn, kThreads, smd, A));
+  } else {
+    TDGL_GCK(ck.kernel((const void*)kg_stencil<T, D3>, nb, kThreads, 0, A));
+    TDGL_GCK(ck.kernel((const void*)kg_dots<T>, nb, kThreads, 0, A));
+    TDGL_GCK(ck.kernel((const void*)kg_fin_dots<T>, 1, kThreads, fin_smem, A));
+    TDGL_GCK(ck.kernel((const void*)kg_orth<T, D3>, nb, kThreads, 0, A));
+    TDGL_GCK(ck.kernel((const void*)kg_fin_orth<T>, 1, kThreads, 0, A));
+  }
   TDGL_GCK(cudaGraphInstantiate(out_exec, G, 0));
   return cudaSuccess;
 }

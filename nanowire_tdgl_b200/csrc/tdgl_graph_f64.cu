@@ -9,4 +9,23 @@ cudaError_t graph_build_f64(const GArgs<double>& A, cudaGraph_t* graph, cudaGrap
   return build_trap_graph<double, false>(A, graph, exec);
 }
 
+// Diagnostic: `launches` standalone Arnoldi steps (orthogonalisation, product, projections).
+cudaError_t arnoldi_probe_f64(const GArgs<double>& A, int launches, cudaStream_t s) {
+  const size_t smo = (size_t)(A.kmax + 1) * sizeof(double);
+  const size_t smd = (size_t)kWarps * (A.kmax + 2) * sizeof(double);
+  cudaError_t e = cudaFuncSetAttribute((const void*)kg_arn_orth<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smo);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute((const void*)kg_arn_dots<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smd);
+  const dim3 grid(A.arn_gx, A.arn_gy, A.g.is3d ? A.g.nz : 1);
+  for (int r = 0; r < launches && e == cudaSuccess; ++r) {
+    kg_arn_orth<double><<<A.nblk_orth, kThreads, smo, s>>>(A);
+    if (A.g.is3d) kg_arn_apply<double, true><<<grid, kThreads, 0, s>>>(A);
+    else kg_arn_apply<double, false><<<grid, kThreads, 0, s>>>(A);
+    kg_arn_dots<double><<<A.nblk_arn, kThreads, smd, s>>>(A);
+    e = cudaGetLastError();
+  }
+  return e;
+}
+
 }  // namespace tdgl
