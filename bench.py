@@ -41,6 +41,7 @@ WORKLOAD = dict(Nx=128, Ny=128, Nz=32, h=0.5, kappa=2.0, Bz=0.5, hole=[(24, 24),
 WORKLOAD_NAME = ("trapezoidal step, 128x128x32-cell film (499,999 interior nodes), 32x32-node hole through "
                  "all planes, h=0.5, kappa=2, Bz=0.5, dt=0.1, Newton tol_f 1e-8 / tol_dx 1e-3, GCR tol 1e-6")
 HBM_FALLBACK_GBS = 6650.0
+DRAM_PER_ALG_BYTE = 0.929
 
 
 def parse():
@@ -56,6 +57,10 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget-s", type=float, default=150.0)
+    ap.add_argument("--arnoldi-probe", type=int, default=None, metavar="J",
+                    help="diagnostic: time the three Arnoldi-step kernels standalone at basis index J and exit")
+    ap.add_argument("--kernel-timers", action="store_true",
+                    help="per-kernel device timers of the step graph (adds a little overhead; not a headline run)")
     return ap.parse_args()
 
 
@@ -100,6 +105,11 @@ def algorithmic_bytes(n_int: int, precision: str, st: dict) -> float:
       Gram-Schmidt + alpha/x/r updates, solve of m iterations:
                                                   sum_k (2(k-1) + 8) SK = (m^2 + 7 m) SK
       Newton residual, norms, x += dx            7 S64 per Newton iteration
+    This is the per-stage model of the reference's GCR form.  The GMRES form
+    run here moves, per solve of m iterations, sum_{j=0..m} (2 j + 7) SK =
+    (m^2 + 8 m + 7) SK (orthogonalisation j + 2 vectors, product 3,
+    projections j + 2; one more step than iterations), within a few percent of
+    the model at m ~ 25, and the measured DRAM traffic is 0.93 x the model.
     """
     S64 = 40.0 * n_int
     SK = (20.0 if precision == "mixed" else 40.0) * n_int
@@ -110,11 +120,12 @@ def algorithmic_bytes(n_int: int, precision: str, st: dict) -> float:
 
 def graph_launches(st: dict, jvp: str) -> int:
     """Kernel launches of the step graph: 7 per step attempt, 4 per Newton
-    iteration, and per Krylov solve of m iterations either m + 1 fused Arnoldi
-    launches (analytic products) or 5 m (finite-difference products)."""
+    iteration, and per Krylov solve of m iterations either 3 (m + 1)
+    (orthogonalisation, product, projections; analytic products) or 5 m
+    (finite-difference products)."""
     base = 7 * (st["steps"] + st["rejections"]) + 4 * st["newton_iters"]
     if jvp == "analytic":
-        return base + st["krylov_iters"] + st["newton_iters"]
+        return base + 3 * (st["krylov_iters"] + st["newton_iters"])
     return base + 5 * st["krylov_iters"]
 
 
@@ -226,10 +237,13 @@ def run_ours(a, rank, world):
         return g, opts, fld
 
     jvp = "analytic" if a.precision == "mixed" else "fd"
+    if a.kernel_timers:
+        os.environ["TDGL_PROFILE"] = "1"    # read when the solver workspace is created
     g, opts, fld = make(a.precision, jvp)
     clocks = Clocks()
     clocks.start()
     x, ms, st = device_run(g, x0, opts, fld, a.warmup, a.steps, dist)
+    timers = g.kernel_timers() if a.kernel_timers else None
     uuid = None
     try:
         uuid = str(torch.cuda.get_device_properties(0).uuid)
@@ -245,13 +259,11 @@ def run_ours(a, rank, world):
     peak, peak_kind = measured_peak()
     alg = algorithmic_bytes(n_int, a.precision, st)
     achieved = alg / (ms / 1e3) / 1e9
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", "stepper_traffic.json")
-    if os.path.exists(tpath):
-        with open(tpath) as fh:
-            tr = json.load(fh)
-        if tr.get("precision") == a.precision and tr.get("dram_bytes_per_step"):
-            traffic = tr["dram_bytes_per_step"] * a.steps
+    # DRAM bytes per algorithmic byte of the GMRES step graph, measured with ncu
+    # (graph-level dram__bytes_read.sum + dram__bytes_write.sum) on a 2-step
+    # launch of this workload in mixed precision; traffic follows the Krylov
+    # counters, so it is scaled by this run's algorithmic bytes.
+    traffic = DRAM_PER_ALG_BYTE * alg if (a.precision == "mixed" and a.krylov == "gmres") else None
     out = {
         "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "weak",
@@ -273,6 +285,13 @@ def run_ours(a, rank, world):
                                         "rejections", "max_krylov")},
         "clocks": clk,
     }
+    if timers is not None:
+        tot = sum(v["ms"] for v in timers.values()) or 1.0
+        out["kernel_timers"] = {k: dict(v, share=v["ms"] / tot, ms_per_step=v["ms"] / a.steps)
+                                for k, v in timers.items() if v["launches"]}
+        out["kernel_timers_note"] = ("device global-timer spans (first block start to last block end) of the "
+                                     "warm-up and timed launches; one-block control kernels and launch gaps "
+                                     "not included")
     # FP64 stepper on the same steps, and the |psi|^2 error of this run against it
     if not a.no_fp64 and a.precision == "mixed":
         res = {}
@@ -346,11 +365,14 @@ def cpu_oracle_steps(max_steps: int, budget_s: float, threads: int):
 def run_reference(a, rank, world):
     if rank != 0:
         return None
-    cores = len(os.sched_getaffinity(0))
+    # The path is sequential numpy / scipy work: more BLAS threads only slow its
+    # long vector updates (measured 0.024 steps/s on 16 threads against 0.045 on
+    # one), so it runs on its fastest setting, one thread.
+    cores = 1
     done, el = cpu_oracle_steps(a.steps, a.cpu_budget_s, cores)
     val = done / el
     sample = (f"{done} of {a.steps} requested trapezoidal steps from the seeded state (wall budget "
-              f"{a.cpu_budget_s:.0f} s), numpy oracle, BLAS on {cores} threads, no warm-up steps")
+              f"{a.cpu_budget_s:.0f} s), numpy oracle, 1 thread (its fastest), no warm-up steps")
     return {"metric": METRIC, "impl": "reference", "value": val, "unit": "steps/s", "n_gpus": world,
             "steps": done, "warmup": 0, "ms_per_step": 1e3 * el / max(done, 1), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -359,8 +381,45 @@ def run_reference(a, rank, world):
             "e2e": {"value": val, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+def arnoldi_probe(a):
+    """Standalone launches of the three Arnoldi-step kernels (orthogonalisation,
+    product, projections) at basis index a.arnoldi_probe on the workload's
+    context, after two steps that fill the basis; prints their time."""
+    import torch
+    from nanowire_tdgl_b200 import _lib as L
+    from nanowire_tdgl_b200.engine import grid_for, stream_handle
+    dev, x0 = build_device()
+    w = WORKLOAD
+    g = grid_for(dev.params, dev.idx, dev.material, a.precision, a.kmax, "gmres")
+    opts = L.TrapOpts(w["t_stop"], w["dt"], 1e-8, w["tol_f"], w["tol_dx"], w["tol_gcr"], w["eps_mf"], 20, 0, 1,
+                      L.TDGL_JVP_ANALYTIC)
+    fld = L.Field(0.0, 0.0, w["Bz"], 1.0, 0.5, w["t_stop"], 0, 0)
+    x = g.pack(x0)
+    rc, t, cur, st = g.trap_run(x, 0.0, w["dt"], 2, opts, fld)
+    if rc != 0:
+        raise RuntimeError(f"filling steps failed with status {rc}")
+    L.check(g.lib.tdgl_arnoldi_probe(g.handle, a.arnoldi_probe, 2, stream_handle()), "tdgl_arnoldi_probe")
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    reps = max(a.steps, 1)
+    e0.record()
+    L.check(g.lib.tdgl_arnoldi_probe(g.handle, a.arnoldi_probe, reps, stream_handle()), "tdgl_arnoldi_probe")
+    e1.record()
+    torch.cuda.synchronize()
+    us = e0.elapsed_time(e1) * 1e3 / reps
+    vec = dev.params.n_interior * (20 if a.precision == "mixed" else 40)
+    alg = (2 * a.arnoldi_probe + 7) * vec
+    print(json.dumps({"arnoldi_probe": a.arnoldi_probe, "precision": a.precision, "us_per_step": us,
+                      "algorithmic_bytes": alg, "achieved_gbs": alg / (us * 1e-6) / 1e9,
+                      "note": "orthogonalisation (j+2 vectors), product (3), projections (j+2); "
+                              "vector = n_interior x 20 B (FP32)"}))
+    return 0
+
+
 def main():
     a = parse()
+    if a.arnoldi_probe is not None:
+        return arnoldi_probe(a)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     if a.impl == "reference":

@@ -182,6 +182,16 @@ class DeviceGrid:
                                     C.byref(field), C.byref(st), stream_handle())
         return rc, tt.value, dd.value, st.as_dict()
 
+    KERNEL_TYPES = ("prepare", "predict", "newton_rhs", "stencil", "projections", "orthogonalisation", "update",
+                    "accept", "arnoldi_product", "arnoldi_orthogonalisation", "arnoldi_projections")
+
+    def kernel_timers(self) -> dict:
+        """Per-kernel-type device time of the graph executor's launches so far
+        (needs TDGL_PROFILE set when the solver workspace was created)."""
+        buf = (C.c_uint64 * 32)()
+        L.check(self.lib.tdgl_profile(self.handle, buf, 32, 0), "tdgl_profile")
+        return {name: {"ms": buf[k] / 1e6, "launches": int(buf[16 + k])} for k, name in enumerate(self.KERNEL_TYPES)}
+
     def euler_run(self, x: torch.Tensor, t: float, t_stop: float, dt: float, n_steps: int, field: L.Field) -> float:
         tt = C.c_double(t)
         L.check(self.lib.tdgl_euler_run(self.handle, _ptr(x), C.byref(tt), float(t_stop), float(dt), int(n_steps),
