@@ -148,6 +148,17 @@ int tdgl_unpack(tdgl_ctx* ctx, const double* x_dev, double* x_ref, tdgl_stream_t
  * with the applied field (Bx, By, Bz) placed as build_boundary_field_vectors does. */
 int tdgl_rhs(tdgl_ctx* ctx, const double* x_dev, double* f_dev, double Bx, double By, double Bz,
              tdgl_stream_t stream);
+/* Adjoint of tdgl_rhs at x (device layout, FP64, any context precision):
+ * gx = J(x)^T v with J = d f / d x (device layout, overwritten);
+ * gsc[d] = d(v . f)/d sc at interior node d (device order; zero without a
+ * material map; may be NULL); gk2[d] = d(v . f)/d kappa(d)^2 (may be NULL);
+ * gpar = d(v . f)/d(Bx, By, Bz, kappa) (4 doubles, may be NULL; the kappa
+ * entry is for a uniform kappa and 0 with per-node kappa).  Adds the
+ * differentiation form the reference lacks: it is the hand-derived reverse
+ * pass of eval_f (src/tdgl3d/physics/rhs.py:147-239) including the
+ * boundary procedure (rhs.py:54-139). */
+int tdgl_vjp(tdgl_ctx* ctx, const double* x_dev, const double* v_dev, double Bx, double By, double Bz,
+             double* gx_dev, double* gsc_dev, double* gk2_dev, double* gpar_dev, tdgl_stream_t stream);
 /* eval_f on reference-layout device buffers (pack, RHS, unpack). */
 int tdgl_eval_f(tdgl_ctx* ctx, const double* x_ref, double* f_ref, double Bx, double By, double Bz,
                 tdgl_stream_t stream);

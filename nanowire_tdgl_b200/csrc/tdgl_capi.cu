@@ -15,6 +15,7 @@
 #include "tdgl_kernels.cuh"
 #include "tdgl_stepper.cuh"
 #include "tdgl_graph.cuh"
+#include "tdgl_adjoint.cuh"
 
 using namespace tdgl;
 
@@ -117,6 +118,9 @@ struct tdgl_ctx {
   unsigned* ticket = nullptr;
   int nblk_arn = 0, nblk_orth = 0, arn_gx = 0, arn_gy = 0;
   uint8_t* imask = nullptr;
+  // adjoint scratch (allocated on first use)
+  double* vjp_part = nullptr;   // 3 x vjp blocks
+  double* vjp_k2 = nullptr;     // n
   std::vector<void*> owned;
 };
 
@@ -249,6 +253,53 @@ extern "C" int tdgl_rhs(tdgl_ctx* c, const double* x, double* f, double Bx, doub
   if (!c || !x || !f) return fail(TDGL_EINVAL, "null argument");
   k_rhs<<<grid_1d(c, c->g.n), kThreads, 0, s>>>(c->g, x, f, bterms(c->g, Bx, By, Bz));
   TDGL_CUDA(cudaGetLastError());
+  return TDGL_OK;
+}
+
+namespace {
+// Sum of the per-block field partials and the uniform-kappa gradient
+// (d/dkappa = 2 kappa sum_m d/dkappa^2(m)), fixed order, one block.
+__global__ void k_vjp_finish(const double* part, int nblk, const double* gk2, int n, double kappa, double* out) {
+  __shared__ double s[4];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int q = warp; q < 4; q += kWarps) {
+    double a = 0.0;
+    if (q < 3) {
+      for (int b = lane; b < nblk; b += 32) a += part[(long)q * nblk + b];
+    } else {
+      for (int d = lane; d < n; d += 32) a += gk2[d];
+    }
+    a = warp_sum(a);
+    if (lane == 0) s[q] = a;
+  }
+  __syncthreads();
+  if (threadIdx.x < 3) out[threadIdx.x] = s[threadIdx.x];
+  if (threadIdx.x == 3) out[3] = 2.0 * kappa * s[3];
+}
+}  // namespace
+
+extern "C" int tdgl_vjp(tdgl_ctx* c, const double* x, const double* v, double Bx, double By, double Bz, double* gx,
+                        double* gsc, double* gk2, double* gpar, tdgl_stream_t s) {
+  if (!c || !x || !v || !gx) return fail(TDGL_EINVAL, "null argument");
+  const Grid& g = c->g;
+  const int nb = grid_1d(c, g.n);
+  int rc;
+  if (!c->vjp_part) {
+    if ((rc = ctx_alloc(c, (void**)&c->vjp_part, sizeof(double) * 3 * (size_t)nb))) return rc;
+    if ((rc = ctx_alloc(c, (void**)&c->vjp_k2, sizeof(double) * (size_t)g.n))) return rc;
+  }
+  double* k2 = gk2 ? gk2 : c->vjp_k2;
+  TDGL_CUDA(cudaMemsetAsync(gx, 0, sizeof(double) * c->L, s));
+  if (gsc && !g.has_material) TDGL_CUDA(cudaMemsetAsync(gsc, 0, sizeof(double) * g.n, s));
+  const BTerms<double> b = bterms(g, Bx, By, Bz);
+  if (g.is3d) k_vjp<true><<<nb, kThreads, 0, s>>>(g, x, v, b, gx, g.has_material ? gsc : nullptr, k2, c->vjp_part);
+  else k_vjp<false><<<nb, kThreads, 0, s>>>(g, x, v, b, gx, g.has_material ? gsc : nullptr, k2, c->vjp_part);
+  TDGL_CUDA(cudaGetLastError());
+  if (gpar) {
+    const double kappa = g.kappa_per_node ? 0.0 : std::sqrt(g.kappa2);
+    k_vjp_finish<<<1, kThreads, 0, s>>>(c->vjp_part, nb, k2, g.n, kappa, gpar);
+    TDGL_CUDA(cudaGetLastError());
+  }
   return TDGL_OK;
 }
 

@@ -182,6 +182,18 @@ class DeviceGrid:
                                     C.byref(field), C.byref(st), stream_handle())
         return rc, tt.value, dd.value, st.as_dict()
 
+    def vjp(self, x: torch.Tensor, v: torch.Tensor, B=(0.0, 0.0, 0.0), want_sc: bool = True):
+        """Adjoint of :meth:`rhs` at x (device layout): returns (J^T v,
+        d(v.f)/d sc per node [device order, or None], d(v.f)/d kappa^2 per node,
+        d(v.f)/d(Bx, By, Bz, kappa))."""
+        gx = torch.empty_like(x)
+        gsc = torch.empty(self.n, dtype=torch.float64, device=self.device) if want_sc else None
+        gk2 = torch.empty(self.n, dtype=torch.float64, device=self.device)
+        gpar = torch.empty(4, dtype=torch.float64, device=self.device)
+        L.check(self.lib.tdgl_vjp(self.handle, _ptr(x), _ptr(v), *map(float, B), _ptr(gx), _ptr(gsc), _ptr(gk2),
+                                  _ptr(gpar), stream_handle()), "tdgl_vjp")
+        return gx, gsc, gk2, gpar
+
     KERNEL_TYPES = ("prepare", "predict", "newton_rhs", "stencil", "projections", "orthogonalisation", "update",
                     "accept", "arnoldi_product", "arnoldi_orthogonalisation", "arnoldi_projections")
 
