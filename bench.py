@@ -57,6 +57,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget-s", type=float, default=150.0)
+    ap.add_argument("--form", choices=["precision", "adjoint"], default="precision",
+                    help="adjoint: gradients of the 64x64x16 differentiation workload instead of the step rate")
     ap.add_argument("--arnoldi-probe", type=int, default=None, metavar="J",
                     help="diagnostic: time the three Arnoldi-step kernels standalone at basis index J and exit")
     ap.add_argument("--kernel-timers", action="store_true",
@@ -420,8 +422,87 @@ def arnoldi_probe(a):
     return 0
 
 
+ADJ = dict(Nx=64, Ny=64, Nz=16, h=0.5, kappa=2.0, Bz=0.4, dt=0.1, n_steps=400, checkpoint=50, seed=5,
+           box=(24, 40, 24, 40, 0, 17))
+
+
+def adjoint_workload():
+    """The differentiation workload: 64x64x16 film, kappa 2, Bz 0.4, a smooth
+    seeded suppression field s(x) in [0, 0.05] (sc = 1 - s; with the
+    reference's -(1 - sc) psi / 0.1 relaxation a larger s drives psi to zero),
+    seeded psi0."""
+    import nanowire_tdgl_b200 as tb
+    w = ADJ
+    p = tb.SimulationParameters(Nx=w["Nx"], Ny=w["Ny"], Nz=w["Nz"], hx=w["h"], hy=w["h"], hz=w["h"],
+                                kappa=w["kappa"])
+    idx = tb.construct_indices(p)
+    rng = np.random.default_rng(w["seed"])
+    z = rng.standard_normal((w["Nz"] + 1, w["Ny"] + 1, w["Nx"] + 1))
+    for _ in range(6):                        # smooth: repeated 3-point averages along each axis
+        for ax in range(3):
+            z = (np.roll(z, 1, ax) + z + np.roll(z, -1, ax)) / 3.0
+    s_full = 0.05 * (z - z.min()) / (z.max() - z.min())
+    sc_full = (1.0 - s_full).reshape(-1)
+    def material(kappa=w["kappa"]):
+        return tb.MaterialMap(kappa=np.full(p.dim_x, kappa), sc_mask=sc_full.copy(),
+                              interior_sc_mask=sc_full[np.asarray(idx.interior_to_full)].copy())
+    n = p.n_interior
+    x0 = np.zeros(p.n_state, dtype=np.complex128)
+    x0[:n] = (1.0 + 0.01 * (rng.standard_normal(n) + 1j * rng.standard_normal(n))) * material().interior_sc_mask
+    return p, idx, material, x0
+
+
+def run_adjoint(a):
+    """Gradient of mean |psi|^2 over the centred box after 400 steps with
+    respect to s(x), Bz and kappa; FP32 Krylov forward (mixed) with the FP64
+    adjoint, timed; central differences (eps 1e-4) of a tight FP64 forward
+    check the Bz and kappa entries of a tight FP64 gradient."""
+    import torch
+    import nanowire_tdgl_b200 as tb
+    w = ADJ
+    p, idx, material, x0 = adjoint_workload()
+    t_stop = w["n_steps"] * w["dt"]
+    loss = tb.box_mean_psi2(p, w["box"])
+    kw = dict(material=material(), B=(0.0, 0.0, w["Bz"]), checkpoint_every=w["checkpoint"])
+    tb.trapezoidal_gradient(x0, p, idx, 0.0, 2 * w["dt"], w["dt"], loss, precision="mixed", **kw)   # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    res = tb.trapezoidal_gradient(x0, p, idx, 0.0, t_stop, w["dt"], loss, precision="mixed",
+                                  newton_tol_f=1e-8, newton_tol_dx=1e-3, tol_gcr=1e-6, **kw)
+    torch.cuda.synchronize()
+    el = time.perf_counter() - t0
+    tight = dict(newton_tol_f=1e-12, newton_tol_dx=1e-10, tol_gcr=1e-11, newton_max_iter=30, kmax=128,
+                 adjoint_tol=1e-11)
+    ref = tb.trapezoidal_gradient(x0, p, idx, 0.0, t_stop, w["dt"], loss, precision="fp64", **kw, **tight)
+    eps = 1e-4
+    def L(kappa=w["kappa"], bz=w["Bz"]):
+        kk = dict(kw, material=material(kappa), B=(0.0, 0.0, bz))
+        pp = p if kappa == w["kappa"] else tb.SimulationParameters(Nx=w["Nx"], Ny=w["Ny"], Nz=w["Nz"], hx=w["h"],
+                                                                    hy=w["h"], hz=w["h"], kappa=kappa)
+        return tb.trapezoidal_gradient(x0, pp, idx, 0.0, t_stop, w["dt"], loss, precision="fp64", backward=False,
+                                       **kk, **tight)["loss"]
+    fd_bz = (L(bz=w["Bz"] + eps) - L(bz=w["Bz"] - eps)) / (2 * eps)
+    fd_k = (L(kappa=w["kappa"] + eps) - L(kappa=w["kappa"] - eps)) / (2 * eps)
+    gs = res["grad_sc"].cpu().numpy()
+    return {"form": "adjoint", "workload": "64x64x16 film (59,535 interior nodes), kappa 2, Bz 0.4, smooth s(x) in "
+                                           "[0, 0.05], loss mean |psi|^2 over the centred 16x16x16 box after 400 "
+                                           "steps dt 0.1, checkpoints every 50",
+            "seconds": el, "steps": res["steps"], "adjoint_gmres_iters": res["adjoint_iters"],
+            "loss": res["loss"], "grad_Bz": float(res["grad_B"][2]), "grad_kappa": res["grad_kappa"],
+            "grad_s_norm": float(np.linalg.norm(gs)),
+            "fp64_grad_Bz": float(ref["grad_B"][2]), "fp64_grad_kappa": ref["grad_kappa"],
+            "fd_grad_Bz": fd_bz, "fd_grad_kappa": fd_k,
+            "rel_err_Bz_vs_fd": abs(float(ref["grad_B"][2]) - fd_bz) / abs(fd_bz),
+            "rel_err_kappa_vs_fd": abs(ref["grad_kappa"] - fd_k) / abs(fd_k),
+            "rel_err_mixed_vs_fp64_Bz": abs(float(res["grad_B"][2]) - float(ref["grad_B"][2]))
+                                        / abs(float(ref["grad_B"][2]))}
+
+
 def main():
     a = parse()
+    if a.form == "adjoint":
+        print(json.dumps(run_adjoint(a)), flush=True)
+        return 0
     if a.arnoldi_probe is not None:
         return arnoldi_probe(a)
     rank = int(os.environ.get("RANK", "0"))

@@ -27,3 +27,6 @@ from .solution import Solution
 
 __all__ += ["DeviceRHS", "FieldSchedule", "eval_f", "forward_euler", "make_eval_f", "newton_gcr_trap",
             "solve", "tgcr_matrix_free_trap", "trapezoidal", "Solution"]
+from .adjoint import box_mean_psi2, rhs, trapezoidal_gradient
+
+__all__ += ["box_mean_psi2", "rhs", "trapezoidal_gradient"]

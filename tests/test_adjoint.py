@@ -83,3 +83,27 @@ def test_vjp_kernel_matches_autograd(name):
         gs = _perm_dev_to_ref(grid, gsc).cpu().numpy()
         r = sct.grad.numpy()
         assert np.max(np.abs(gs - r)) < 1e-11 * max(np.max(np.abs(r)), 1.0)
+
+
+@pytest.mark.gpu
+def test_autograd_function_matches_torch_reference():
+    import nanowire_tdgl_b200 as tb
+    d = golden("case_3d_hole")
+    dev = device_from_fixture(d)
+    g = orc.make_grid(dev.params, dev.idx, dev.material)
+    rng = np.random.default_rng(3)
+    x = torch.tensor(tr.to_real(d["X_seeded"], g))
+    w = torch.tensor(rng.standard_normal(x.numel()))
+    B = [torch.tensor(v, dtype=torch.float64, requires_grad=True) for v in (0.05, -0.1, 0.3)]
+    xa = x.clone().requires_grad_(True)
+    fa = tb.rhs(xa.cuda(), dev.params, dev.idx, dev.material, B)
+    (fa.cpu() * w).sum().backward()
+    xb = x.clone().requires_grad_(True)
+    Bb = [b.detach().clone().requires_grad_(True) for b in B]
+    sc = None if g.sc_int is None else torch.tensor(g.sc_int)
+    fb = tr.eval_f(g, xb, sc, *Bb)
+    assert torch.allclose(fa.cpu(), fb, rtol=0, atol=1e-12 * float(fb.abs().max()))
+    (fb * w).sum().backward()
+    assert torch.allclose(xa.grad, xb.grad, rtol=0, atol=1e-11 * float(xb.grad.abs().max()))
+    for a, b in zip(B, Bb):
+        assert abs(float(a.grad) - float(b.grad)) <= 1e-10 * max(abs(float(b.grad)), 1.0)
