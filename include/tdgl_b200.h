@@ -192,6 +192,22 @@ int tdgl_newton_trap(tdgl_ctx* ctx, double* x_dev, const double* gamma_dev, doub
  * loop of trapezoidal (src/tdgl3d/solvers/integrators.py:150-197). */
 int tdgl_trap_run(tdgl_ctx* ctx, double* x_dev, double* t, double* dt_cur, int32_t max_steps,
                   const tdgl_trap_opts* opts, const tdgl_field* field, tdgl_stats* stats, tdgl_stream_t stream);
+/* tdgl_trap_run in two halves, for stepping many contexts concurrently (the
+ * batched form; no reference counterpart): tdgl_trap_launch enqueues the
+ * steps on the stream and returns at once (GMRES contexts only; x must stay
+ * valid until the stream has passed them); after the stream has completed,
+ * tdgl_trap_collect returns the clock, step size, counters and status.  One
+ * uncollected launch per context at a time. */
+int tdgl_trap_launch(tdgl_ctx* ctx, double* x_dev, double t, double dt_cur, int32_t max_steps,
+                     const tdgl_trap_opts* opts, const tdgl_field* field, tdgl_stream_t stream);
+int tdgl_trap_collect(tdgl_ctx* ctx, double* t, double* dt_cur, tdgl_stats* stats);
+/* Launch shape of the step graph's grid kernels: block counts, each in
+ * [1, 8 x SMs], of the grid-stride passes and of the Arnoldi streams (defaults
+ * 8 and 5 blocks per SM).  Any count gives a correct step; reductions are
+ * deterministic for a given count.  Used by the batched form's autotuner
+ * (small instances run concurrently on few blocks each); the graph is rebuilt
+ * at the next launch.  No reference counterpart. */
+int tdgl_ctx_set_blocks(tdgl_ctx* ctx, int32_t stream_blocks, int32_t krylov_blocks);
 /* Forward Euler: n_steps steps of min(dt, t_stop - t) from *t (updated)
  * (src/tdgl3d/solvers/integrators.py:35-89). */
 int tdgl_euler_run(tdgl_ctx* ctx, double* x_dev, double* t, double t_stop, double dt, int32_t n_steps,

@@ -30,3 +30,6 @@ __all__ += ["DeviceRHS", "FieldSchedule", "eval_f", "forward_euler", "make_eval_
 from .adjoint import box_mean_psi2, rhs, trapezoidal_gradient
 
 __all__ += ["box_mean_psi2", "rhs", "trapezoidal_gradient"]
+from .batch import BatchedTrapezoidal
+
+__all__ += ["BatchedTrapezoidal"]

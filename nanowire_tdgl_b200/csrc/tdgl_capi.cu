@@ -31,6 +31,8 @@ cudaError_t arnoldi_probe_f64(const GArgs<double>& A, int launches, cudaStream_t
 }  // namespace tdgl
 
 static constexpr long kProfLen = 64 + 2 * 1024;
+// upper bound of the step graph's blocks per SM (its partial-sum buffers are sized for it)
+static constexpr int kMaxBlocksPerSm = 8;
 
 namespace {
 
@@ -117,20 +119,36 @@ struct tdgl_ctx {
   double* part_arn = nullptr;
   unsigned* ticket = nullptr;
   int nblk_arn = 0, nblk_orth = 0, arn_gx = 0, arn_gy = 0;
+  int blk_stream = 0, blk_krylov = 0;   // blocks of the graph's grid kernels (0: defaults)
+  bool pending = false, pending_noop = false;   // an uncollected tdgl_trap_launch
   uint8_t* imask = nullptr;
   // adjoint scratch (allocated on first use)
   double* vjp_part = nullptr;   // 3 x vjp blocks
   double* vjp_k2 = nullptr;     // n
   std::vector<void*> owned;
+  bool unsettled = false;       // initialisation memsets / copies not yet known complete
 };
 
+// Zero-filled device buffer owned by the context.  The fill (and the pageable
+// host copies of initial contents) run on the legacy default stream, which
+// work on a non-blocking stream does not wait for: settle() ends every
+// function that allocates, before work on the caller's stream may use it.
 static int ctx_alloc(tdgl_ctx* c, void** p, size_t bytes) {
   cudaError_t e = cudaMalloc(p, bytes);
   if (e != cudaSuccess) return fail(TDGL_ENOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
   c->owned.push_back(*p);
   c->bytes += bytes;
+  c->unsettled = true;
   e = cudaMemset(*p, 0, bytes);
   if (e != cudaSuccess) return fail(TDGL_ECUDA, std::string("cudaMemset: ") + cudaGetErrorString(e));
+  return TDGL_OK;
+}
+
+static int settle(tdgl_ctx* c) {
+  if (!c->unsettled) return TDGL_OK;
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) return fail(TDGL_ECUDA, std::string("initialising buffers: ") + cudaGetErrorString(e));
+  c->unsettled = false;
   return TDGL_OK;
 }
 
@@ -207,6 +225,7 @@ extern "C" int tdgl_ctx_create(const tdgl_grid_desc* gd, const tdgl_material_des
   if ((rc = ctx_alloc(c, (void**)&c->s_red, 64 * sizeof(double)))) { tdgl_ctx_destroy(c); return rc; }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) { tdgl_ctx_destroy(c); return fail(TDGL_ECUDA, cudaGetErrorString(e)); }
+  if ((rc = settle(c))) { tdgl_ctx_destroy(c); return rc; }
   *out = c;
   return TDGL_OK;
 }
@@ -287,6 +306,7 @@ extern "C" int tdgl_vjp(tdgl_ctx* c, const double* x, const double* v, double Bx
   if (!c->vjp_part) {
     if ((rc = ctx_alloc(c, (void**)&c->vjp_part, sizeof(double) * 3 * (size_t)nb))) return rc;
     if ((rc = ctx_alloc(c, (void**)&c->vjp_k2, sizeof(double) * (size_t)g.n))) return rc;
+    if ((rc = settle(c))) return rc;
   }
   double* k2 = gk2 ? gk2 : c->vjp_k2;
   TDGL_CUDA(cudaMemsetAsync(gx, 0, sizeof(double) * c->L, s));
@@ -403,7 +423,7 @@ static int ensure_workspace(tdgl_ctx* c) {
     if ((rc = ctx_alloc(c, (void**)&c->prof, kProfLen * sizeof(unsigned long long)))) return rc;
   TDGL_CUDA(cudaMallocHost((void**)&c->ctl_host, sizeof(Ctl)));
   c->ws_ready = true;
-  return TDGL_OK;
+  return settle(c);
 }
 
 template <typename T>
@@ -602,16 +622,12 @@ static int ensure_arnoldi_ws(tdgl_ctx* c) {
   const size_t vb = (size_t)g.ncomp * c->npf * tsz;
   c->arn_gx = (g.nx + 31) / 32;
   c->arn_gy = (g.ny + 7) / 8;
-  const char* eb = std::getenv("TDGL_DOTS_BLOCKS_PER_SM");
-  // streaming kernels of the step, resident at 5 blocks per SM (their register budgets)
-  c->nblk_arn = c->num_sms * (eb && std::atoi(eb) > 0 ? std::atoi(eb) : 5);
-  const char* eo = std::getenv("TDGL_ORTH_BLOCKS_PER_SM");
-  c->nblk_orth = std::min(c->gblocks, c->num_sms * (eo && std::atoi(eo) > 0 ? std::atoi(eo) : 5));
   int rc;
   if ((rc = ctx_alloc(c, &c->UB, vb * (c->kmax + 1)))) return rc;
   if ((rc = ctx_alloc(c, &c->Zb[0], vb))) return rc;
   if ((rc = ctx_alloc(c, &c->Zb[1], vb))) return rc;
-  if ((rc = ctx_alloc(c, (void**)&c->part_arn, sizeof(double) * (c->kmax + 2) * (size_t)c->nblk_arn))) return rc;
+  if ((rc = ctx_alloc(c, (void**)&c->part_arn, sizeof(double) * (c->kmax + 2) * (size_t)c->num_sms * kMaxBlocksPerSm)))
+    return rc;
   if ((rc = ctx_alloc(c, (void**)&c->ticket, sizeof(unsigned)))) return rc;
   // interior mask of the full grid (projections run over interior entries only)
   std::vector<uint8_t> im((size_t)c->npf, 0);
@@ -632,12 +648,23 @@ static int ensure_graph(tdgl_ctx* c, int v) {
     const Grid& g = c->g;
     long dimx = g.is3d ? (long)g.mk * (g.Nz + 1) : (long)g.mk;
     c->npf = (dimx + 127) / 128 * 128;
-    const char* es = std::getenv("TDGL_STREAM_BLOCKS_PER_SM");
-    c->gblocks = c->num_sms * (es && std::atoi(es) > 0 ? std::atoi(es) : 8);
+    // grid kernels of the step: 8 blocks per SM for the one-node-per-thread
+    // passes, 5 for the Arnoldi streams (their register budgets), unless set by
+    // tdgl_ctx_set_blocks or TDGL_STREAM_BLOCKS_PER_SM / TDGL_KRYLOV_BLOCKS_PER_SM
+    auto env_bps = [](const char* name, int dflt) {
+      const char* e = std::getenv(name);
+      const int v = e ? std::atoi(e) : 0;
+      return (v >= 1 && v <= kMaxBlocksPerSm) ? v : dflt;
+    };
+    if (!c->blk_stream) c->blk_stream = c->num_sms * env_bps("TDGL_STREAM_BLOCKS_PER_SM", 8);
+    if (!c->blk_krylov) c->blk_krylov = c->num_sms * env_bps("TDGL_KRYLOV_BLOCKS_PER_SM", 5);
+    c->gblocks = c->blk_stream;
+    c->nblk_arn = c->blk_krylov;
+    c->nblk_orth = std::min(c->gblocks, c->nblk_arn);
     const size_t tsz = c->precision == TDGL_MIXED ? sizeof(float) : sizeof(double);
     const size_t full64 = (size_t)g.ncomp * c->npf * sizeof(double);
     const size_t fullT = (size_t)g.ncomp * c->npf * tsz;
-    const size_t nb = (size_t)c->gblocks;
+    const size_t nb = (size_t)c->num_sms * kMaxBlocksPerSm;
     if ((rc = ctx_alloc(c, (void**)&c->Xn, c->L * sizeof(double)))) return rc;
     if ((rc = ctx_alloc(c, (void**)&c->En, full64))) return rc;
     if ((rc = ctx_alloc(c, (void**)&c->Ei, full64))) return rc;
@@ -675,7 +702,7 @@ static int ensure_graph(tdgl_ctx* c, int v) {
     c->gexec[v] = nullptr;
     return fail(TDGL_ECUDA, std::string("building the stepper graph: ") + cudaGetErrorString(e));
   }
-  return TDGL_OK;
+  return settle(c);
 }
 
 static int graph_status(int gs) {
@@ -689,15 +716,17 @@ static int graph_status(int gs) {
   }
 }
 
-static int run_graph(tdgl_ctx* c, double* x, double* t, double* dt_cur, int32_t max_steps, const tdgl_trap_opts* o,
-                     const tdgl_field* f, tdgl_stats* st, tdgl_stream_t s) {
+// Enqueue one graph launch for up to max_steps steps on stream s (no
+// synchronisation); *noop is set when nothing needs to run.
+static int graph_launch(tdgl_ctx* c, double* x, double t0, double cur0, int32_t max_steps, const tdgl_trap_opts* o,
+                        const tdgl_field* f, tdgl_stream_t s, bool* noop) {
   int rc;
   const int v = o->jvp_mode == TDGL_JVP_ANALYTIC ? 1 : 0;
   if ((rc = ensure_graph(c, v))) return rc;
   GDev& h = *c->gdev_host;
   std::memset(&h, 0, sizeof(GDev));
-  h.t = *t;
-  h.dt_cur = *dt_cur;
+  h.t = t0;
+  h.dt_cur = cur0;
   h.t_stop = o->t_stop;
   h.dt = o->dt;
   h.dt_min = o->dt_min;
@@ -721,20 +750,27 @@ static int run_graph(tdgl_ctx* c, double* x, double* t, double* dt_cur, int32_t 
   h.watchdog_cap = (long long)(max_steps + 1) * 40 * (o->newton_max_iter + 2) * (c->kmax + 3) + 1000;
   h.prof_on = c->gprof ? 1 : 0;
   for (int k = 0; k < kKTypes; ++k) h.kt_start[k] = ~0ull;
-  if (tdgl_stats* z = st) std::memset(z, 0, sizeof(*z));
-  if (!(h.t < h.t_stop - 1e-14) || max_steps <= 0) {
-    if (st) { st->t = h.t; st->dt_cur = h.dt_cur; }
-    return TDGL_OK;
-  }
+  *noop = !(h.t < h.t_stop - 1e-14) || max_steps <= 0;
+  if (*noop) return TDGL_OK;
   TDGL_CUDA(cudaMemcpyAsync(c->Xn, x, c->L * sizeof(double), cudaMemcpyDeviceToDevice, s));
   TDGL_CUDA(cudaMemcpyAsync(c->gdev, &h, sizeof(GDev), cudaMemcpyHostToDevice, s));
   if (c->ticket) TDGL_CUDA(cudaMemsetAsync(c->ticket, 0, sizeof(unsigned), s));
   TDGL_CUDA(cudaGraphLaunch(c->gexec[v], s));
   TDGL_CUDA(cudaMemcpyAsync(&h, c->gdev, sizeof(GDev), cudaMemcpyDeviceToHost, s));
   TDGL_CUDA(cudaMemcpyAsync(x, c->Xn, c->L * sizeof(double), cudaMemcpyDeviceToDevice, s));
-  TDGL_CUDA(cudaStreamSynchronize(s));
+  return TDGL_OK;
+}
+
+// Results of the last graph_launch once its stream has completed.
+static int graph_collect(tdgl_ctx* c, bool noop, double* t, double* dt_cur, tdgl_stats* st) {
+  GDev& h = *c->gdev_host;
+  if (tdgl_stats* z = st) std::memset(z, 0, sizeof(*z));
   *t = h.t;
   *dt_cur = h.dt_cur;
+  if (noop) {
+    if (st) { st->t = h.t; st->dt_cur = h.dt_cur; }
+    return TDGL_OK;
+  }
   for (int k = 0; k < kKTypes; ++k) {
     c->gk_total[k] += h.kt_total[k];
     c->gk_count[k] += h.kt_count[k];
@@ -759,6 +795,56 @@ static int run_graph(tdgl_ctx* c, double* x, double* t, double* dt_cur, int32_t 
     st->kernel_launches = 1;
   }
   return graph_status(h.status);
+}
+
+static int run_graph(tdgl_ctx* c, double* x, double* t, double* dt_cur, int32_t max_steps, const tdgl_trap_opts* o,
+                     const tdgl_field* f, tdgl_stats* st, tdgl_stream_t s) {
+  bool noop = false;
+  int rc = graph_launch(c, x, *t, *dt_cur, max_steps, o, f, s, &noop);
+  if (rc) return rc;
+  if (!noop) TDGL_CUDA(cudaStreamSynchronize(s));
+  return graph_collect(c, noop, t, dt_cur, st);
+}
+
+extern "C" int tdgl_trap_launch(tdgl_ctx* c, double* x, double t, double dt_cur, int32_t max_steps,
+                                const tdgl_trap_opts* o, const tdgl_field* f, tdgl_stream_t s) {
+  if (!c || !x || !o || !f) return fail(TDGL_EINVAL, "null argument");
+  if (o->jvp_mode == TDGL_JVP_FD && c->precision == TDGL_MIXED)
+    return fail(TDGL_EINVAL, "the finite-difference product needs the FP64 context");
+  if (c->krylov != KRY_GMRES) return fail(TDGL_EINVAL, "asynchronous stepping needs the GMRES graph executor");
+  if (c->pending) return fail(TDGL_EINVAL, "a launch of this context has not been collected");
+  int rc = graph_launch(c, x, t, dt_cur, max_steps, o, f, s, &c->pending_noop);
+  if (rc == TDGL_OK) c->pending = true;
+  return rc;
+}
+
+extern "C" int tdgl_trap_collect(tdgl_ctx* c, double* t, double* dt_cur, tdgl_stats* st) {
+  if (!c || !t || !dt_cur) return fail(TDGL_EINVAL, "null argument");
+  if (!c->pending) return fail(TDGL_EINVAL, "no launch to collect");
+  c->pending = false;
+  return graph_collect(c, c->pending_noop, t, dt_cur, st);
+}
+
+extern "C" int tdgl_ctx_set_blocks(tdgl_ctx* c, int32_t stream_blocks, int32_t krylov_blocks) {
+  if (!c) return fail(TDGL_EINVAL, "null argument");
+  const int cap = c->num_sms * kMaxBlocksPerSm;
+  if (stream_blocks < 1 || stream_blocks > cap || krylov_blocks < 1 || krylov_blocks > cap)
+    return fail(TDGL_EINVAL, "block counts must lie in [1, 8 x SMs]");
+  if (c->pending) return fail(TDGL_EINVAL, "a launch of this context has not been collected");
+  c->blk_stream = stream_blocks;
+  c->blk_krylov = krylov_blocks;
+  if (c->gws_ready) {
+    c->gblocks = c->blk_stream;
+    c->nblk_arn = c->blk_krylov;
+    c->nblk_orth = std::min(c->gblocks, c->nblk_arn);
+  }
+  for (int v = 0; v < 2; ++v) {           // rebuilt with the new shapes at the next launch
+    if (c->gexec[v]) cudaGraphExecDestroy(c->gexec[v]);
+    if (c->graph[v]) cudaGraphDestroy(c->graph[v]);
+    c->gexec[v] = nullptr;
+    c->graph[v] = nullptr;
+  }
+  return TDGL_OK;
 }
 
 extern "C" int tdgl_trap_run(tdgl_ctx* c, double* x, double* t, double* dt_cur, int32_t max_steps,

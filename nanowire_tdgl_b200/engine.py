@@ -204,6 +204,25 @@ class DeviceGrid:
         L.check(self.lib.tdgl_profile(self.handle, buf, 32, 0), "tdgl_profile")
         return {name: {"ms": buf[k] / 1e6, "launches": int(buf[16 + k])} for k, name in enumerate(self.KERNEL_TYPES)}
 
+    def trap_launch(self, x: torch.Tensor, t: float, dt_cur: float, max_steps: int, opts: L.TrapOpts,
+                    field: L.Field, stream: torch.cuda.Stream) -> None:
+        """Enqueue up to max_steps steps on ``stream`` (returns at once)."""
+        L.check(self.lib.tdgl_trap_launch(self.handle, _ptr(x), float(t), float(dt_cur), int(max_steps),
+                                          C.byref(opts), C.byref(field), C.c_void_p(stream.cuda_stream)),
+                "tdgl_trap_launch")
+
+    def trap_collect(self) -> tuple[int, float, float, dict]:
+        """Results of the last trap_launch (its stream must have completed)."""
+        tt, dd = C.c_double(0.0), C.c_double(0.0)
+        st = L.Stats()
+        rc = self.lib.tdgl_trap_collect(self.handle, C.byref(tt), C.byref(dd), C.byref(st))
+        return rc, tt.value, dd.value, st.as_dict()
+
+    def set_blocks(self, stream_blocks: int, krylov_blocks: int) -> None:
+        """Block counts of the step graph's grid-stride and Arnoldi kernels."""
+        L.check(self.lib.tdgl_ctx_set_blocks(self.handle, int(stream_blocks), int(krylov_blocks)),
+                "tdgl_ctx_set_blocks")
+
     def euler_run(self, x: torch.Tensor, t: float, t_stop: float, dt: float, n_steps: int, field: L.Field) -> float:
         tt = C.c_double(t)
         L.check(self.lib.tdgl_euler_run(self.handle, _ptr(x), C.byref(tt), float(t_stop), float(dt), int(n_steps),

@@ -1,0 +1,107 @@
+"""Batched form: instances stepped concurrently give exactly the states of
+stepping them one after another with the same launch shapes; stream
+assignment and block-count rules checked on the host."""
+
+import numpy as np
+import pytest
+
+
+def _instances(n=5, seed=0):
+    import nanowire_tdgl_b200 as tb
+    rng = np.random.default_rng(seed)
+    devs, xs = [], []
+    for q in range(n):
+        Nx, Ny = (int(v) for v in rng.choice([12, 16, 20, 24], 2))
+        Nz = int(rng.choice([1, 4, 6]))
+        p = tb.SimulationParameters(Nx=Nx, Ny=Ny, Nz=Nz, hx=0.5, hy=0.5, hz=0.5, kappa=float(rng.uniform(1.5, 4)))
+        d = tb.Device(p, applied_field=tb.AppliedField(Bz=float(rng.uniform(0.1, 1.0)), t_on_fraction=1.0))
+        if q % 2:
+            i0, j0 = int(rng.integers(3, Nx - 8)), int(rng.integers(3, Ny - 8))
+            s = int(rng.integers(3, 6))
+            d.add_hole([(0.5 * i0, 0.5 * j0), (0.5 * (i0 + s), 0.5 * j0), (0.5 * (i0 + s), 0.5 * (j0 + s)),
+                        (0.5 * i0, 0.5 * (j0 + s))])
+        x = d.initial_state()
+        m = x.psi.shape[0]
+        x.psi[:] += 0.02 * (rng.standard_normal(m) + 1j * rng.standard_normal(m))
+        devs.append(d)
+        xs.append(x.data.copy())
+    return devs, xs
+
+
+def test_stream_assignment_balances_work():
+    from nanowire_tdgl_b200.batch import assign_streams
+    sizes = [135375, 2883, 50000, 50000, 9000, 120000, 4000, 60000]
+    queues, order = assign_streams(sizes, 3)
+    assert sorted(i for q in queues for i in q) == list(range(len(sizes)))
+    assert sorted(i for _, i in order) == list(range(len(sizes)))
+    loads = [sum(sizes[i] for i in q) for q in queues]
+    assert max(loads) <= sum(sizes) / 3 + max(sizes)
+    assert queues[0][0] == 0                        # largest first
+    assert [i for _, i in order[:3]] == [q[0] for q in queues]   # first of every stream first
+    assert all(order.index((s, q[r])) < order.index((s, q[r + 1])) for s, q in enumerate(queues)
+               for r in range(len(q) - 1))
+    assert len(assign_streams(sizes, 100)[0]) == len(sizes)
+
+
+def test_block_rule():
+    from nanowire_tdgl_b200.batch import launch_blocks
+    assert launch_blocks(10_000, None, 148) == (8 * 148, 5 * 148)
+    assert launch_blocks(2883, 1, 148) == (12, 8)
+    assert launch_blocks(2883, 16, 148) == (1, 1)
+    assert launch_blocks(10 ** 8, 1, 148) == (8 * 148, 5 * 148)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+@pytest.mark.parametrize("shape", [None, 2])
+def test_batched_equals_sequential(precision, shape):
+    import nanowire_tdgl_b200 as tb
+    devs, xs = _instances()
+    a = tb.BatchedTrapezoidal(devs, xs, 0.1, precision=precision, kmax=96, n_streams=3)
+    a.set_shape(shape)
+    a.step(3)
+    sa = a.states()
+    ta, tot_a = list(a.t), dict(a.totals)
+    b = tb.BatchedTrapezoidal(devs, xs, 0.1, precision=precision, kmax=96)
+    b.set_shape(shape)
+    b.step_sequential(3)
+    for u, v in zip(sa, b.states()):
+        assert np.array_equal(u, v)
+    assert ta == b.t and tot_a == b.totals
+    assert all(abs(t - 0.3) < 1e-12 for t in ta)
+
+
+@pytest.mark.gpu
+def test_small_launch_shape_matches_default_within_tolerance():
+    """Other block counts change only the reduction partition: tightly
+    converged states agree with the default shape's to rounding."""
+    import nanowire_tdgl_b200 as tb
+    devs, xs = _instances(3, seed=2)
+    kw = dict(precision="fp64", kmax=96, newton_tol_f=1e-12, newton_tol_dx=1e-10, tol_gcr=1e-11)
+    a = tb.BatchedTrapezoidal(devs, xs, 0.1, **kw)
+    a.set_shape(None)
+    a.step(2)
+    sa = a.states()
+    a2 = tb.BatchedTrapezoidal(devs, xs, 0.1, **kw)
+    a2.set_shape(16)
+    a2.step(2)
+    for u, v in zip(sa, a2.states()):
+        assert np.max(np.abs(u - v)) < 1e-9
+
+
+@pytest.mark.gpu
+def test_autotune_keeps_a_candidate_and_restores_states():
+    import nanowire_tdgl_b200 as tb
+    devs, xs = _instances(4, seed=1)
+    a = tb.BatchedTrapezoidal(devs, xs, 0.1, kmax=96)
+    x_before = [x.clone() for x in a.x]
+    times = a.autotune((None, 4), steps=1)
+    assert a.best in times and a.shape == a.best
+    assert all(np.array_equal(u.cpu().numpy(), v.cpu().numpy()) for u, v in zip(x_before, a.x))
+    assert a.t == [0.0] * 4 and a.totals["steps"] == 0
+    a.step(2)
+    b = tb.BatchedTrapezoidal(devs, xs, 0.1, kmax=96)
+    b.set_shape(a.best)
+    b.step_sequential(2)
+    for u, v in zip(a.states(), b.states()):
+        assert np.array_equal(u, v)
