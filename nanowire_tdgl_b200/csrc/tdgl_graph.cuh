@@ -671,15 +671,17 @@ __global__ void __launch_bounds__(kThreads) kg_accept(GArgs<T> A) {
 // ---------------------------------------------------------------------------
 //
 // Step ja of a Krylov solve runs
-//   kg_arn_orth   U_ja = Z_{ja-1} - sum_{i<ja} gam_i U_i   (nothing for ja = 0: U_0 = r0,
-//                 written by the Newton residual)
+//   kg_arn_orth   U_ja = s_{ja-1} (Z_{ja-1} - sum_{i<ja} gam_i U_i)   (nothing for ja = 0:
+//                 U_0 = r0, written by the Newton residual)
 //   kg_arn_apply  Z_ja = U_ja - dt/2 J(x) U_ja  (A U_ja; the tangent-linear product is
 //                 linear)
 //   kg_arn_dots   <Z_ja, U_i> (i <= ja) over the interior entries (||U_ja||^2 comes
 //                 with the orthogonalisation).
 // The basis stays unnormalised (v_i = s_i U_i, s_i = 1 / ||U_i||): with
 // gam_i = s_i^2 <Z_{ja-1}, U_i>, U_ja is the classical Gram-Schmidt remainder of
-// A v_{ja-1} divided by s_{ja-1}.  The last block of kg_arn_dots adds the
+// A v_{ja-1}, so ||U_ja|| = h_{ja,ja-1} stays of the order of ||A|| (without the
+// factor s_{ja-1} the norms would multiply from one vector to the next and
+// leave the FP32 range within a few dozen iterations of a stiff system).  The last block of kg_arn_dots adds the
 // partials in a fixed order, completes Hessenberg column ja-1 (norm, Givens
 // rotation, residual estimate and the stop test of tgcr.py:125, 141-142) and,
 // when the iteration goes on, stores column ja and the next coefficients.  A
@@ -706,7 +708,7 @@ __device__ void arn_finish(const GArgs<T>& A, GDev* d, int ja, const double* S) 
     double* sn = kry_sn(A);
     double* col = kry_H(A) + (long)(jc - 1) * (A.kmax + 1);
     const double un = sqrt(S[ja + 1]);
-    const double hn = un * sj[jc - 1];                   // h_{jc, jc-1} = ||A v - sum h v||
+    const double hn = un;                                // h_{jc, jc-1} = ||A v - sum h v|| = ||U_jc||
     sj[jc] = un > 0.0 ? 1.0 / un : 0.0;
     d->jvp_evals += 1;
     col[jc] = hn;
@@ -782,8 +784,9 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 5 : 3) kg_arn_orth(
   const int ja = d->ja;
   if (ja == 0) return;
   kt_begin(d, KT_ARN_ORTH);
-  extern __shared__ double gsm[];              // gam_0 .. gam_{ja-1}
-  for (int t = threadIdx.x; t < ja; t += blockDim.x) gsm[t] = kry_gam(A)[t];
+  extern __shared__ double gsm[];              // s_{ja-1} gam_0 .. s_{ja-1} gam_{ja-1}
+  const double sc = kry_sj(A)[ja - 1];
+  for (int t = threadIdx.x; t < ja; t += blockDim.x) gsm[t] = sc * kry_gam(A)[t];
   __syncthreads();
   const T* Zin = A.Zb[(ja + 1) & 1];
   T* Uj = A.UB + (long)ja * A.vs;
@@ -795,7 +798,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 5 : 3) kg_arn_orth(
   for (; q < nq; q += stride) {
     const long e = 4 * q;
     const V4<T> z = ld4(Zin + e);
-    double v[4] = {(double)z.a, (double)z.b, (double)z.c, (double)z.d};
+    double v[4] = {sc * (double)z.a, sc * (double)z.b, sc * (double)z.c, sc * (double)z.d};
     const T* U = A.UB + e;
     int i = 0;
     for (; i + 4 <= ja; i += 4) {

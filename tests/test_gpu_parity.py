@@ -235,3 +235,24 @@ def test_fused_arnoldi_across_tiles(tb, periodic):
     mixed = tb.solve(dev, **{**kw, "precision": "mixed"})
     p64 = np.abs(fused.psi(-1)) ** 2
     assert np.linalg.norm(np.abs(mixed.psi(-1)) ** 2 - p64) / np.linalg.norm(p64) < 1e-6
+
+
+@pytest.mark.parametrize("kappa", [3.0, 4.0])
+def test_mixed_precision_stiff_kappa(tb, kappa):
+    """Large kappa^2 dt / h^2 (a stiff phi block, long Krylov solves): the
+    FP32 Arnoldi basis stays in range and the mixed stepper tracks FP64."""
+    p = tb.SimulationParameters(Nx=20, Ny=12, Nz=4, hx=0.5, hy=0.5, hz=0.5, kappa=kappa)
+    dev = tb.Device(p, applied_field=tb.AppliedField(Bz=0.6, t_on_fraction=1.0))
+    dev.add_hole([(3.0, 2.0), (5.0, 2.0), (5.0, 4.0), (3.0, 4.0)])
+    x0 = dev.initial_state()
+    rng = np.random.default_rng(7)
+    n = x0.psi.shape[0]
+    x0.psi += 0.01 * (rng.standard_normal(n) + 1j * rng.standard_normal(n)) * dev.material.interior_sc_mask
+    kw = dict(t_start=0.0, t_stop=0.5, dt=0.1, method="trapezoidal", x0=x0, progress=False, log_metadata=False,
+              newton_tol_f=1e-8, newton_tol_dx=1e-3, tol_gcr=1e-6)
+    ref = tb.solve(dev, precision="fp64", **kw)
+    mix = tb.solve(dev, precision="mixed", **kw)
+    assert np.array_equal(ref.times, mix.times)
+    p_ref = np.abs(ref.psi(-1)) ** 2
+    p_mix = np.abs(mix.psi(-1)) ** 2
+    assert np.linalg.norm(p_mix - p_ref) / np.linalg.norm(p_ref) < 1e-6
