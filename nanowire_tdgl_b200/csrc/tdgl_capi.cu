@@ -118,6 +118,10 @@ struct tdgl_ctx {
   void* Zb[2] = {nullptr, nullptr};
   double* part_arn = nullptr;
   unsigned* ticket = nullptr;
+  int ntiles = 0, ngroups = 0;   // tiles of the product-and-projections kernel, groups of 32 tiles
+  double* gpart = nullptr;
+  unsigned* gticket = nullptr;
+  int apply_dots = 1;            // product and projections fused (TDGL_ARN_APPLY_DOTS=0: separate kernels)
   int nblk_arn = 0, nblk_orth = 0, arn_gx = 0, arn_gy = 0;
   int blk_stream = 0, blk_krylov = 0;   // blocks of the graph's grid kernels (0: defaults)
   bool pending = false, pending_noop = false;   // an uncollected tdgl_trap_launch
@@ -607,6 +611,11 @@ static GArgs<T> make_gargs(tdgl_ctx* c) {
   A.nblk_orth = c->nblk_orth;
   A.arn_gx = c->arn_gx;
   A.arn_gy = c->arn_gy;
+  A.apply_dots = c->apply_dots;
+  A.ntiles = c->ntiles;
+  A.ngroups = c->ngroups;
+  A.gpart = c->gpart;
+  A.gticket = c->gticket;
   A.imask = c->imask;
   A.cxu = c->g.kappa2 / c->g.hx2;
   A.cyu = c->g.kappa2 / c->g.hy2;
@@ -622,12 +631,18 @@ static int ensure_arnoldi_ws(tdgl_ctx* c) {
   const size_t vb = (size_t)g.ncomp * c->npf * tsz;
   c->arn_gx = (g.nx + 31) / 32;
   c->arn_gy = (g.ny + 7) / 8;
+  c->ntiles = c->arn_gx * c->arn_gy * (g.is3d ? g.nz : 1);
+  c->ngroups = (c->ntiles + 31) / 32;
+  const char* ead = std::getenv("TDGL_ARN_APPLY_DOTS");
+  c->apply_dots = !(ead && ead[0] == '0');
   int rc;
   if ((rc = ctx_alloc(c, &c->UB, vb * (c->kmax + 1)))) return rc;
   if ((rc = ctx_alloc(c, &c->Zb[0], vb))) return rc;
   if ((rc = ctx_alloc(c, &c->Zb[1], vb))) return rc;
-  if ((rc = ctx_alloc(c, (void**)&c->part_arn, sizeof(double) * (c->kmax + 2) * (size_t)c->num_sms * kMaxBlocksPerSm)))
-    return rc;
+  const size_t nparts = std::max((size_t)c->num_sms * kMaxBlocksPerSm, (size_t)c->ntiles);
+  if ((rc = ctx_alloc(c, (void**)&c->part_arn, sizeof(double) * (c->kmax + 2) * nparts))) return rc;
+  if ((rc = ctx_alloc(c, (void**)&c->gpart, sizeof(double) * (c->kmax + 2) * (size_t)c->ngroups))) return rc;
+  if ((rc = ctx_alloc(c, (void**)&c->gticket, sizeof(unsigned) * (size_t)c->ngroups))) return rc;
   if ((rc = ctx_alloc(c, (void**)&c->ticket, sizeof(unsigned)))) return rc;
   // interior mask of the full grid (projections run over interior entries only)
   std::vector<uint8_t> im((size_t)c->npf, 0);
@@ -755,6 +770,7 @@ static int graph_launch(tdgl_ctx* c, double* x, double t0, double cur0, int32_t 
   TDGL_CUDA(cudaMemcpyAsync(c->Xn, x, c->L * sizeof(double), cudaMemcpyDeviceToDevice, s));
   TDGL_CUDA(cudaMemcpyAsync(c->gdev, &h, sizeof(GDev), cudaMemcpyHostToDevice, s));
   if (c->ticket) TDGL_CUDA(cudaMemsetAsync(c->ticket, 0, sizeof(unsigned), s));
+  if (c->gticket) TDGL_CUDA(cudaMemsetAsync(c->gticket, 0, sizeof(unsigned) * (size_t)c->ngroups, s));
   TDGL_CUDA(cudaGraphLaunch(c->gexec[v], s));
   TDGL_CUDA(cudaMemcpyAsync(&h, c->gdev, sizeof(GDev), cudaMemcpyDeviceToHost, s));
   TDGL_CUDA(cudaMemcpyAsync(x, c->Xn, c->L * sizeof(double), cudaMemcpyDeviceToDevice, s));

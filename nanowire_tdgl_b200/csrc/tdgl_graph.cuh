@@ -119,6 +119,12 @@ struct GArgs {
   const uint8_t* imask;   // full grid: 1 at interior nodes
   double cxu, cyu, czu;   // uniform kappa^2 / h^2 (node_coef's values without a per-node kappa)
   int standalone;      // diagnostic launch outside the graph: no bookkeeping, no conditionals
+  // product and projections in one kernel (kg_arn_apply_dots): per-tile partials
+  // [(kmax + 1) x ntiles] in part_arn, group partials [(kmax + 1) x ngroups]
+  int apply_dots;      // 1: kg_arn_apply_dots; 0: kg_arn_apply then kg_arn_dots
+  int ntiles, ngroups;
+  double* gpart;
+  unsigned* gticket;   // [ngroups] arrival counters
 };
 
 template <typename T> __host__ __device__ __forceinline__ double* kry_sj(const GArgs<T>& A) { return A.kry; }
@@ -959,6 +965,166 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 5 : 4) kg_arn_dots(
       d->kt_total[KT_ARN_DOTS] += global_ns() - d->kt_start[KT_ARN_DOTS];
       d->kt_count[KT_ARN_DOTS] += 1;
       d->kt_start[KT_ARN_DOTS] = ~0ull;
+    }
+  }
+}
+
+// Product and projections in one kernel: each block computes Z_ja = A U_ja
+// on its 32 x 8 tile of one plane (the stencil of kg_arn_apply) and, with the
+// tile's Z values still in registers, the tile's share of <Z_ja, U_i> for
+// i <= ja (reading U_i at the same nodes).  Blocks are scheduled in waves, so
+// stencil arithmetic of some blocks overlaps the basis reads of others, and
+// Z_ja is not read back.  Per tile and vector, each thread's product goes to
+// shared memory and one warp sums the block's 256 products in double; the tile
+// sums are folded in two fixed-order levels (groups of kTileGroup tiles, then
+// the groups) by the last block of each group and the last group, which does
+// the column bookkeeping (arn_finish).
+constexpr int kTileGroup = 32;
+template <typename T> struct ProdChunk { static constexpr int VC = 16; };   // vectors per shared-memory pass
+
+// Dynamic shared memory of kg_arn_apply_dots: the products of one pass, and
+// (last block) the kmax + 2 folded sums.
+template <typename T>
+__host__ __device__ inline size_t apply_dots_smem(int kmax) {
+  const size_t prod = (size_t)ProdChunk<T>::VC * kThreads * sizeof(T);
+  const size_t sums = (size_t)(kmax + 2) * sizeof(double);
+  return prod > sums ? prod : sums;
+}
+
+template <typename T, bool D3>
+__global__ void __launch_bounds__(kThreads, 3) kg_arn_apply_dots(GArgs<T> A) {
+  GDev* d = A.dev;
+  if (!gdev_ok(d)) {
+    if (blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x == 0) abort_all(A, d->status);
+    return;
+  }
+  kt_begin(d, KT_ARN_APPLY);
+  constexpr int NC = D3 ? 5 : 4;
+  constexpr int VC = ProdChunk<T>::VC;
+  const Grid& g = A.g;
+  const int ja = d->ja;
+  const long npf = A.npf;
+  const T* Uj = A.UB + (long)ja * A.vs;
+  T* Zout = A.Zb[ja & 1];
+  const double dth = d->dta / 2.0;
+  const int i = 1 + blockIdx.x * 32 + (threadIdx.x & 31), j = 1 + blockIdx.y * 8 + (threadIdx.x >> 5);
+  const int k = D3 ? 1 + (int)blockIdx.z : 0;
+  const bool inside = i <= g.nx && j <= g.ny;
+  const long m = full_index(g, i, j, k);
+  T zt[NC];
+#pragma unroll
+  for (int c = 0; c < NC; ++c) zt[c] = T(0);
+  if (inside) {
+    const int n = dix(g, i, j, k);
+    const uint8_t nf = g.nflags[n];
+    NodeCoef<T> nc;
+    if (g.kappa_per_node) nc = node_coef<T>(g, n, nf);
+    else {
+      nc.cx = (T)A.cxu; nc.cy = (T)A.cyu; nc.cz = (T)A.czu;
+      nc.material = g.has_material != 0;
+      if (!nc.material) nc.sc = T(1);
+      else if (nf & NF_SCFRAC) nc.sc = (T)g.scint[n];
+      else nc.sc = (nf & NF_SC0) ? T(0) : T(1);
+    }
+    NbE<T, T> X{A.XLe, npf, m, g.mj, g.mk};
+    NbM<T> P{Uj, npf, m, g.mj, g.mk, i, j, k, &g, g.lflags};
+    T o[5];
+    jvp_body<T, D3>(g, X, P, nc, nf, o);
+    double z[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      z[c] = (double)Uj[c * npf + m] - dth * (double)o[c];
+      zt[c] = (T)z[c];
+    }
+    write_eff<T, D3, true>(g, Zout, npf, i, j, k, z, 0.0, 0.0, 0.0);
+  }
+  // projections of this tile
+  extern __shared__ __align__(16) unsigned char psm[];
+  T* pv = reinterpret_cast<T*>(psm);                 // [VC][kThreads] per-thread products
+  __shared__ bool last;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int tile = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+  const int ntiles = A.ntiles;
+  for (int c0 = 0; c0 <= ja; c0 += VC) {
+    const int nv = min(VC, ja + 1 - c0);
+    for (int t0 = 0; t0 < nv; t0 += 4) {
+      T u[4][NC];
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const T* U = A.UB + (long)(c0 + t0 + t) * A.vs + m;
+        const bool ok = inside && t0 + t < nv;
+#pragma unroll
+        for (int c = 0; c < NC; ++c) u[t][c] = ok ? U[c * npf] : T(0);
+      }
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        T pr = T(0);
+#pragma unroll
+        for (int c = 0; c < NC; ++c) pr += zt[c] * u[t][c];
+        if (t0 + t < nv) pv[(t0 + t) * kThreads + threadIdx.x] = pr;
+      }
+    }
+    __syncthreads();
+    for (int v = warp; v < nv; v += kWarps) {
+      double a = 0.0;
+#pragma unroll
+      for (int r = 0; r < kThreads / 32; ++r) a += (double)pv[v * kThreads + r * 32 + lane];
+      a = warp_sum(a);
+      if (lane == 0) A.part_arn[(long)(c0 + v) * ntiles + tile] = a;
+    }
+    __syncthreads();
+  }
+  // level 1: the last block of each group of kTileGroup tiles sums the group
+  __threadfence();
+  __syncthreads();
+  const int grp = tile / kTileGroup, g0 = grp * kTileGroup;
+  const int gs = min(kTileGroup, ntiles - g0);
+  if (threadIdx.x == 0) last = atomicAdd(A.gticket + grp, 1u) == (unsigned)gs - 1;
+  __syncthreads();
+  if (!last) {
+    kt_end(d, KT_ARN_APPLY);
+    return;
+  }
+  __threadfence();
+  for (int s2 = warp; s2 <= ja; s2 += kWarps) {
+    double a = lane < gs ? __ldcg(A.part_arn + (long)s2 * ntiles + g0 + lane) : 0.0;
+    a = warp_sum(a);
+    if (lane == 0) A.gpart[(long)s2 * A.ngroups + grp] = a;
+  }
+  if (threadIdx.x == 0) A.gticket[grp] = 0u;
+  // level 2: the last group sums the groups and does the bookkeeping
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(A.ticket, 1u) == (unsigned)A.ngroups - 1;
+  __syncthreads();
+  if (!last) {
+    kt_end(d, KT_ARN_APPLY);
+    return;
+  }
+  __threadfence();
+  double* S = reinterpret_cast<double*>(psm);
+  for (int s2 = warp; s2 < ja + 2; s2 += kWarps) {
+    double a = 0.0;
+    if (s2 <= ja) {
+      for (int bb = lane; bb < A.ngroups; bb += 32) a += __ldcg(A.gpart + (long)s2 * A.ngroups + bb);
+    } else if (ja > 0) {       // ||U_ja||^2 from the orthogonalisation's partials
+      for (int bb = lane; bb < A.nblk_orth; bb += 32) a += __ldcg(A.part_orth + bb);
+    }
+    a = warp_sum(a);
+    if (lane == 0) S[s2] = a;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    *A.ticket = 0u;
+    if (A.standalone) return;
+    if (d->status != GS_OK) { abort_all(A, d->status); return; }
+    kt_fold(d, KT_ARN_ORTH);
+    arn_finish(A, d, ja, S);
+    if (d->prof_on) {
+      d->kt_total[KT_ARN_APPLY] += global_ns() - d->kt_start[KT_ARN_APPLY];
+      d->kt_count[KT_ARN_APPLY] += 1;
+      d->kt_start[KT_ARN_APPLY] = ~0ull;
+      d->kt_end[KT_ARN_APPLY] = 0;
     }
   }
 }

@@ -85,9 +85,16 @@ cudaError_t build_trap_graph(GArgs<T> A, cudaGraph_t* out_graph, cudaGraphExec_t
     TDGL_GCK(cudaFuncSetAttribute((const void*)kg_arn_orth<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smo));
     TDGL_GCK(cudaFuncSetAttribute((const void*)kg_arn_dots<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smd));
     TDGL_GCK(ck.kernel((const void*)kg_arn_orth<T>, A.nblk_orth, kThreads, smo, A));
-    TDGL_GCK(ck.kernel((const void*)kg_arn_apply<T, D3>, dim3(A.arn_gx, A.arn_gy, D3 ? A.g.nz : 1), kThreads, 0,
-                       A));
-    TDGL_GCK(ck.kernel((const void*)kg_arn_dots<T>, A.nblk_arn, kThreads, smd, A));
+    const dim3 tiles(A.arn_gx, A.arn_gy, D3 ? A.g.nz : 1);
+    if (A.apply_dots) {
+      const size_t smp = apply_dots_smem<T>(A.kmax);
+      TDGL_GCK(cudaFuncSetAttribute((const void*)kg_arn_apply_dots<T, D3>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smp));
+      TDGL_GCK(ck.kernel((const void*)kg_arn_apply_dots<T, D3>, tiles, kThreads, smp, A));
+    } else {
+      TDGL_GCK(ck.kernel((const void*)kg_arn_apply<T, D3>, tiles, kThreads, 0, A));
+      TDGL_GCK(ck.kernel((const void*)kg_arn_dots<T>, A.nblk_arn, kThreads, smd, A));
+    }
   } else {
     TDGL_GCK(ck.kernel((const void*)kg_stencil<T, D3>, nb, kThreads, 0, A));
     TDGL_GCK(ck.kernel((const void*)kg_dots<T>, nb, kThreads, 0, A));

@@ -17,12 +17,24 @@ cudaError_t arnoldi_probe_f32(const GArgs<float>& A, int launches, cudaStream_t 
                                        (int)smo);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute((const void*)kg_arn_dots<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smd);
+  const size_t smp = apply_dots_smem<float>(A.kmax);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute((const void*)kg_arn_apply_dots<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smp);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute((const void*)kg_arn_apply_dots<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smp);
   const dim3 grid(A.arn_gx, A.arn_gy, A.g.is3d ? A.g.nz : 1);
   for (int r = 0; r < launches && e == cudaSuccess; ++r) {
     kg_arn_orth<float><<<A.nblk_orth, kThreads, smo, s>>>(A);
-    if (A.g.is3d) kg_arn_apply<float, true><<<grid, kThreads, 0, s>>>(A);
-    else kg_arn_apply<float, false><<<grid, kThreads, 0, s>>>(A);
-    kg_arn_dots<float><<<A.nblk_arn, kThreads, smd, s>>>(A);
+    if (A.apply_dots) {
+      if (A.g.is3d) kg_arn_apply_dots<float, true><<<grid, kThreads, smp, s>>>(A);
+      else kg_arn_apply_dots<float, false><<<grid, kThreads, smp, s>>>(A);
+    } else {
+      if (A.g.is3d) kg_arn_apply<float, true><<<grid, kThreads, 0, s>>>(A);
+      else kg_arn_apply<float, false><<<grid, kThreads, 0, s>>>(A);
+      kg_arn_dots<float><<<A.nblk_arn, kThreads, smd, s>>>(A);
+    }
     e = cudaGetLastError();
   }
   return e;

@@ -17,12 +17,24 @@ cudaError_t arnoldi_probe_f64(const GArgs<double>& A, int launches, cudaStream_t
                                        (int)smo);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute((const void*)kg_arn_dots<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smd);
+  const size_t smp = apply_dots_smem<double>(A.kmax);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute((const void*)kg_arn_apply_dots<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smp);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute((const void*)kg_arn_apply_dots<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smp);
   const dim3 grid(A.arn_gx, A.arn_gy, A.g.is3d ? A.g.nz : 1);
   for (int r = 0; r < launches && e == cudaSuccess; ++r) {
     kg_arn_orth<double><<<A.nblk_orth, kThreads, smo, s>>>(A);
-    if (A.g.is3d) kg_arn_apply<double, true><<<grid, kThreads, 0, s>>>(A);
-    else kg_arn_apply<double, false><<<grid, kThreads, 0, s>>>(A);
-    kg_arn_dots<double><<<A.nblk_arn, kThreads, smd, s>>>(A);
+    if (A.apply_dots) {
+      if (A.g.is3d) kg_arn_apply_dots<double, true><<<grid, kThreads, smp, s>>>(A);
+      else kg_arn_apply_dots<double, false><<<grid, kThreads, smp, s>>>(A);
+    } else {
+      if (A.g.is3d) kg_arn_apply<double, true><<<grid, kThreads, 0, s>>>(A);
+      else kg_arn_apply<double, false><<<grid, kThreads, 0, s>>>(A);
+      kg_arn_dots<double><<<A.nblk_arn, kThreads, smd, s>>>(A);
+    }
     e = cudaGetLastError();
   }
   return e;
