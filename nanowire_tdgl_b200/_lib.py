@@ -87,7 +87,7 @@ SIGNATURES = {
     "tdgl_euler_run": (C.c_int, [_P, _P, C.POINTER(_D), _D, _D, _I, C.POINTER(Field), _P]),
     "tdgl_vjp": (C.c_int, [_P, _P, _P, _D, _D, _D, _P, _P, _P, _P, _P]),
     "tdgl_profile": (C.c_int, [_P, C.POINTER(C.c_uint64), C.c_int64, _I]),
-    "tdgl_arnoldi_probe": (C.c_int, [_P, _I, _I, _P]),
+    "tdgl_arnoldi_probe": (C.c_int, [_P, _I, _I, _I, _P]),
     "tdgl_eval_f_noalloc": (C.c_int, [C.POINTER(GridDesc), C.POINTER(MaterialDesc), _P, _P, _D, _D, _D, _P]),
 }
 

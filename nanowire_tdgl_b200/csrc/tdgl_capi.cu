@@ -26,8 +26,8 @@ cudaError_t stepper_launch_f32(StepArgs<float> A, int blocks, size_t smem, cudaS
 cudaError_t stepper_launch_f64(StepArgs<double> A, int blocks, size_t smem, cudaStream_t s);
 cudaError_t graph_build_f32(const GArgs<float>& A, cudaGraph_t* graph, cudaGraphExec_t* exec);
 cudaError_t graph_build_f64(const GArgs<double>& A, cudaGraph_t* graph, cudaGraphExec_t* exec);
-cudaError_t arnoldi_probe_f32(const GArgs<float>& A, int launches, cudaStream_t s);
-cudaError_t arnoldi_probe_f64(const GArgs<double>& A, int launches, cudaStream_t s);
+cudaError_t arnoldi_probe_f32(const GArgs<float>& A, int launches, int kernels, cudaStream_t s);
+cudaError_t arnoldi_probe_f64(const GArgs<double>& A, int launches, int kernels, cudaStream_t s);
 }  // namespace tdgl
 
 static constexpr long kProfLen = 64 + 2 * 1024;
@@ -119,6 +119,7 @@ struct tdgl_ctx {
   double* part_arn = nullptr;
   unsigned* ticket = nullptr;
   int ntiles = 0, ngroups = 0;   // tiles of the product-and-projections kernel, groups of 32 tiles
+  int ngroups_cap = 0;           // group-partial slots: groups of tiles or of projection blocks
   double* gpart = nullptr;
   unsigned* gticket = nullptr;
   int apply_dots = 1;            // product and projections fused (TDGL_ARN_APPLY_DOTS=0: separate kernels)
@@ -633,6 +634,7 @@ static int ensure_arnoldi_ws(tdgl_ctx* c) {
   c->arn_gy = (g.ny + 7) / 8;
   c->ntiles = c->arn_gx * c->arn_gy * (g.is3d ? g.nz : 1);
   c->ngroups = (c->ntiles + 31) / 32;
+  c->ngroups_cap = std::max(c->ngroups, (c->num_sms * kMaxBlocksPerSm + 31) / 32);
   const char* ead = std::getenv("TDGL_ARN_APPLY_DOTS");
   c->apply_dots = !(ead && ead[0] == '0');
   int rc;
@@ -641,8 +643,8 @@ static int ensure_arnoldi_ws(tdgl_ctx* c) {
   if ((rc = ctx_alloc(c, &c->Zb[1], vb))) return rc;
   const size_t nparts = std::max((size_t)c->num_sms * kMaxBlocksPerSm, (size_t)c->ntiles);
   if ((rc = ctx_alloc(c, (void**)&c->part_arn, sizeof(double) * (c->kmax + 2) * nparts))) return rc;
-  if ((rc = ctx_alloc(c, (void**)&c->gpart, sizeof(double) * (c->kmax + 2) * (size_t)c->ngroups))) return rc;
-  if ((rc = ctx_alloc(c, (void**)&c->gticket, sizeof(unsigned) * (size_t)c->ngroups))) return rc;
+  if ((rc = ctx_alloc(c, (void**)&c->gpart, sizeof(double) * (c->kmax + 2) * (size_t)c->ngroups_cap))) return rc;
+  if ((rc = ctx_alloc(c, (void**)&c->gticket, sizeof(unsigned) * (size_t)c->ngroups_cap))) return rc;
   if ((rc = ctx_alloc(c, (void**)&c->ticket, sizeof(unsigned)))) return rc;
   // interior mask of the full grid (projections run over interior entries only)
   std::vector<uint8_t> im((size_t)c->npf, 0);
@@ -770,7 +772,7 @@ static int graph_launch(tdgl_ctx* c, double* x, double t0, double cur0, int32_t 
   TDGL_CUDA(cudaMemcpyAsync(c->Xn, x, c->L * sizeof(double), cudaMemcpyDeviceToDevice, s));
   TDGL_CUDA(cudaMemcpyAsync(c->gdev, &h, sizeof(GDev), cudaMemcpyHostToDevice, s));
   if (c->ticket) TDGL_CUDA(cudaMemsetAsync(c->ticket, 0, sizeof(unsigned), s));
-  if (c->gticket) TDGL_CUDA(cudaMemsetAsync(c->gticket, 0, sizeof(unsigned) * (size_t)c->ngroups, s));
+  if (c->gticket) TDGL_CUDA(cudaMemsetAsync(c->gticket, 0, sizeof(unsigned) * (size_t)c->ngroups_cap, s));
   TDGL_CUDA(cudaGraphLaunch(c->gexec[v], s));
   TDGL_CUDA(cudaMemcpyAsync(&h, c->gdev, sizeof(GDev), cudaMemcpyDeviceToHost, s));
   TDGL_CUDA(cudaMemcpyAsync(x, c->Xn, c->L * sizeof(double), cudaMemcpyDeviceToDevice, s));
@@ -935,7 +937,7 @@ extern "C" int tdgl_euler_run(tdgl_ctx* c, double* x, double* t, double t_stop, 
   return TDGL_OK;
 }
 
-extern "C" int tdgl_arnoldi_probe(tdgl_ctx* c, int32_t ja, int32_t launches, tdgl_stream_t s) {
+extern "C" int tdgl_arnoldi_probe(tdgl_ctx* c, int32_t ja, int32_t launches, int32_t kernels, tdgl_stream_t s) {
   if (!c || launches < 0) return fail(TDGL_EINVAL, "invalid argument");
   int rc;
   if ((rc = ensure_graph(c, 1))) return rc;
@@ -946,12 +948,12 @@ extern "C" int tdgl_arnoldi_probe(tdgl_ctx* c, int32_t ja, int32_t launches, tdg
     GArgs<float> A = make_gargs<float>(c);
     A.fused = 1;
     A.standalone = 1;
-    e = arnoldi_probe_f32(A, launches, s);
+    e = arnoldi_probe_f32(A, launches, kernels, s);
   } else {
     GArgs<double> A = make_gargs<double>(c);
     A.fused = 1;
     A.standalone = 1;
-    e = arnoldi_probe_f64(A, launches, s);
+    e = arnoldi_probe_f64(A, launches, kernels, s);
   }
   if (e != cudaSuccess) return fail(TDGL_ECUDA, std::string("Arnoldi step launch: ") + cudaGetErrorString(e));
   TDGL_CUDA(cudaStreamSynchronize(s));

@@ -687,10 +687,12 @@ __global__ void __launch_bounds__(kThreads) kg_accept(GArgs<T> A) {
 // gam_i = s_i^2 <Z_{ja-1}, U_i>, U_ja is the classical Gram-Schmidt remainder of
 // A v_{ja-1}, so ||U_ja|| = h_{ja,ja-1} stays of the order of ||A|| (without the
 // factor s_{ja-1} the norms would multiply from one vector to the next and
-// leave the FP32 range within a few dozen iterations of a stiff system).  The last block of kg_arn_dots adds the
-// partials in a fixed order, completes Hessenberg column ja-1 (norm, Givens
-// rotation, residual estimate and the stop test of tgcr.py:125, 141-142) and,
-// when the iteration goes on, stores column ja and the next coefficients.  A
+// leave the FP32 range within a few dozen iterations of a stiff system).
+// The partials are added in a fixed order (the last block of each group of 32
+// blocks sums its group, the last group sums the groups), and that last block
+// completes Hessenberg column ja-1 (norm, Givens rotation, residual estimate
+// and the stop test of tgcr.py:125, 141-142) and, when the iteration goes on,
+// stores column ja and the next coefficients.  A
 // solve of m iterations takes m + 1 steps; the last product is not used.
 //
 // The vectors live on the full grid with their face values, and the boundary
@@ -875,6 +877,68 @@ __global__ void __launch_bounds__(kThreads, 3) kg_arn_apply(GArgs<T> A) {
   kt_end(d, KT_ARN_APPLY);
 }
 
+// Blocks of a two-level fold: groups of kTileGroup consecutive blocks.
+constexpr int kTileGroup = 32;
+
+// Level 1 of the two-level fold of the projections (whole block, after its
+// partials part[s * nb + b] for s <= ja are written): the last block of block
+// b's group to arrive adds the group's partials into gpart[s * ng + group].
+// Returns true in the block that, after that, is the last of all groups.
+template <typename T>
+__device__ bool arn_fold_groups(const GArgs<T>& A, const double* part, int nb, int b, int ja) {
+  __shared__ bool last;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int grp = b / kTileGroup, g0 = grp * kTileGroup;
+  const int gs = min(kTileGroup, nb - g0);
+  const int ng = (nb + kTileGroup - 1) / kTileGroup;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(A.gticket + grp, 1u) == (unsigned)gs - 1;
+  __syncthreads();
+  if (!last) return false;
+  __threadfence();
+  for (int s2 = warp; s2 <= ja; s2 += kWarps) {
+    double a = lane < gs ? __ldcg(part + (long)s2 * nb + g0 + lane) : 0.0;
+    a = warp_sum(a);
+    if (lane == 0) A.gpart[(long)s2 * ng + grp] = a;
+  }
+  if (threadIdx.x == 0) A.gticket[grp] = 0u;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(A.ticket, 1u) == (unsigned)ng - 1;
+  __syncthreads();
+  if (!last) return false;
+  __threadfence();
+  return true;
+}
+
+// Final fold (whole block of the last group): S[s] = sum over the ng group
+// partials for s <= ja, S[ja + 1] = ||U_ja||^2 from the orthogonalisation's
+// nblk_orth partials (ja > 0), all in a fixed order.
+template <typename T>
+__device__ void arn_fold_final(const GArgs<T>& A, int ng, int ja, double* S) {
+  __shared__ double ow[kWarps];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int s2 = warp; s2 <= ja; s2 += kWarps) {
+    double a = 0.0;
+    for (int bb = lane; bb < ng; bb += 32) a += __ldcg(A.gpart + (long)s2 * ng + bb);
+    a = warp_sum(a);
+    if (lane == 0) S[s2] = a;
+  }
+  double o = 0.0;
+  if (ja > 0)
+    for (int bb = threadIdx.x; bb < A.nblk_orth; bb += kThreads) o += __ldcg(A.part_orth + bb);
+  o = warp_sum(o);
+  if (lane == 0) ow[warp] = o;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0;
+    for (int w = 0; w < kWarps; ++w) a += ow[w];
+    S[ja + 1] = a;
+  }
+  __syncthreads();
+}
+
 // Projections <Z_ja, U_i> (i <= ja) over the interior entries (imask), in
 // passes over groups of GGroup<T>::JB vectors whose loads are all in flight
 // together.  A thread's few products per vector are summed in T (the vectors'
@@ -889,7 +953,6 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 5 : 4) kg_arn_dots(
     return;
   }
   kt_begin(d, KT_ARN_DOTS);
-  __shared__ bool last_block;
   extern __shared__ double red[];              // [kWarps][ja + 2]
   const int ja = d->ja;
   const int nd = ja + 2;
@@ -935,25 +998,9 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 5 : 4) kg_arn_dots(
     for (int w = 0; w < kWarps; ++w) a += red[w * nd + s];
     A.part_arn[(long)s * A.nblk_arn + blockIdx.x] = a;
   }
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) last_block = atomicAdd(A.ticket, 1u) == (unsigned)A.nblk_arn - 1;
-  __syncthreads();
-  if (!last_block) return;
-  __threadfence();
-  // fixed-order fold of the partials (L2 reads: other blocks wrote them)
+  if (!arn_fold_groups(A, A.part_arn, A.nblk_arn, blockIdx.x, ja)) return;
   double* S = red;
-  for (int s = warp; s < nd; s += kWarps) {
-    double a = 0.0;
-    if (s <= ja) {
-      for (int bb = lane; bb < A.nblk_arn; bb += 32) a += __ldcg(A.part_arn + (long)s * A.nblk_arn + bb);
-    } else if (ja > 0) {       // ||U_ja||^2 from the orthogonalisation's partials
-      for (int bb = lane; bb < A.nblk_orth; bb += 32) a += __ldcg(A.part_orth + bb);
-    }
-    a = warp_sum(a);
-    if (lane == 0) S[s] = a;
-  }
-  __syncthreads();
+  arn_fold_final(A, (A.nblk_arn + kTileGroup - 1) / kTileGroup, ja, S);
   if (threadIdx.x == 0) {
     *A.ticket = 0u;
     if (A.standalone) return;
@@ -979,7 +1026,6 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 5 : 4) kg_arn_dots(
 // sums are folded in two fixed-order levels (groups of kTileGroup tiles, then
 // the groups) by the last block of each group and the last group, which does
 // the column bookkeeping (arn_finish).
-constexpr int kTileGroup = 32;
 template <typename T> struct ProdChunk { static constexpr int VC = 16; };   // vectors per shared-memory pass
 
 // Dynamic shared memory of kg_arn_apply_dots: the products of one pass, and
@@ -1041,7 +1087,6 @@ __global__ void __launch_bounds__(kThreads, 3) kg_arn_apply_dots(GArgs<T> A) {
   // projections of this tile
   extern __shared__ __align__(16) unsigned char psm[];
   T* pv = reinterpret_cast<T*>(psm);                 // [VC][kThreads] per-thread products
-  __shared__ bool last;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int tile = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
   const int ntiles = A.ntiles;
@@ -1074,46 +1119,12 @@ __global__ void __launch_bounds__(kThreads, 3) kg_arn_apply_dots(GArgs<T> A) {
     }
     __syncthreads();
   }
-  // level 1: the last block of each group of kTileGroup tiles sums the group
-  __threadfence();
-  __syncthreads();
-  const int grp = tile / kTileGroup, g0 = grp * kTileGroup;
-  const int gs = min(kTileGroup, ntiles - g0);
-  if (threadIdx.x == 0) last = atomicAdd(A.gticket + grp, 1u) == (unsigned)gs - 1;
-  __syncthreads();
-  if (!last) {
+  if (!arn_fold_groups(A, A.part_arn, ntiles, tile, ja)) {
     kt_end(d, KT_ARN_APPLY);
     return;
   }
-  __threadfence();
-  for (int s2 = warp; s2 <= ja; s2 += kWarps) {
-    double a = lane < gs ? __ldcg(A.part_arn + (long)s2 * ntiles + g0 + lane) : 0.0;
-    a = warp_sum(a);
-    if (lane == 0) A.gpart[(long)s2 * A.ngroups + grp] = a;
-  }
-  if (threadIdx.x == 0) A.gticket[grp] = 0u;
-  // level 2: the last group sums the groups and does the bookkeeping
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) last = atomicAdd(A.ticket, 1u) == (unsigned)A.ngroups - 1;
-  __syncthreads();
-  if (!last) {
-    kt_end(d, KT_ARN_APPLY);
-    return;
-  }
-  __threadfence();
   double* S = reinterpret_cast<double*>(psm);
-  for (int s2 = warp; s2 < ja + 2; s2 += kWarps) {
-    double a = 0.0;
-    if (s2 <= ja) {
-      for (int bb = lane; bb < A.ngroups; bb += 32) a += __ldcg(A.gpart + (long)s2 * A.ngroups + bb);
-    } else if (ja > 0) {       // ||U_ja||^2 from the orthogonalisation's partials
-      for (int bb = lane; bb < A.nblk_orth; bb += 32) a += __ldcg(A.part_orth + bb);
-    }
-    a = warp_sum(a);
-    if (lane == 0) S[s2] = a;
-  }
-  __syncthreads();
+  arn_fold_final(A, A.ngroups, ja, S);
   if (threadIdx.x == 0) {
     *A.ticket = 0u;
     if (A.standalone) return;

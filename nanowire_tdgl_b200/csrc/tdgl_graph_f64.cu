@@ -9,15 +9,18 @@ cudaError_t graph_build_f64(const GArgs<double>& A, cudaGraph_t* graph, cudaGrap
   return build_trap_graph<double, false>(A, graph, exec);
 }
 
-// Diagnostic: `launches` standalone Arnoldi steps (orthogonalisation, product, projections).
-cudaError_t arnoldi_probe_f64(const GArgs<double>& A, int launches, cudaStream_t s) {
+// Diagnostic: `launches` standalone Arnoldi steps.  kernels: bit 0 the
+// orthogonalisation, bit 1 the product, bit 2 the projections, bit 3 the fused
+// product and projections; 0 = the kernels of this context's graph.
+cudaError_t arnoldi_probe_f64(const GArgs<double>& A, int launches, int kernels, cudaStream_t s) {
   const size_t smo = (size_t)(A.kmax + 1) * sizeof(double);
   const size_t smd = (size_t)kWarps * (A.kmax + 2) * sizeof(double);
+  const size_t smp = apply_dots_smem<double>(A.kmax);
+  if (kernels == 0) kernels = 1 | (A.apply_dots ? 8 : 2 | 4);
   cudaError_t e = cudaFuncSetAttribute((const void*)kg_arn_orth<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smo);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute((const void*)kg_arn_dots<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smd);
-  const size_t smp = apply_dots_smem<double>(A.kmax);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute((const void*)kg_arn_apply_dots<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smp);
@@ -26,14 +29,15 @@ cudaError_t arnoldi_probe_f64(const GArgs<double>& A, int launches, cudaStream_t
                              (int)smp);
   const dim3 grid(A.arn_gx, A.arn_gy, A.g.is3d ? A.g.nz : 1);
   for (int r = 0; r < launches && e == cudaSuccess; ++r) {
-    kg_arn_orth<double><<<A.nblk_orth, kThreads, smo, s>>>(A);
-    if (A.apply_dots) {
-      if (A.g.is3d) kg_arn_apply_dots<double, true><<<grid, kThreads, smp, s>>>(A);
-      else kg_arn_apply_dots<double, false><<<grid, kThreads, smp, s>>>(A);
-    } else {
+    if (kernels & 1) kg_arn_orth<double><<<A.nblk_orth, kThreads, smo, s>>>(A);
+    if (kernels & 2) {
       if (A.g.is3d) kg_arn_apply<double, true><<<grid, kThreads, 0, s>>>(A);
       else kg_arn_apply<double, false><<<grid, kThreads, 0, s>>>(A);
-      kg_arn_dots<double><<<A.nblk_arn, kThreads, smd, s>>>(A);
+    }
+    if (kernels & 4) kg_arn_dots<double><<<A.nblk_arn, kThreads, smd, s>>>(A);
+    if (kernels & 8) {
+      if (A.g.is3d) kg_arn_apply_dots<double, true><<<grid, kThreads, smp, s>>>(A);
+      else kg_arn_apply_dots<double, false><<<grid, kThreads, smp, s>>>(A);
     }
     e = cudaGetLastError();
   }
