@@ -656,6 +656,15 @@ static int ensure_arnoldi_ws(tdgl_ctx* c) {
   return TDGL_OK;
 }
 
+// Block counts of the graph's grid kernels from the stream and Krylov settings:
+// the orthogonalisation runs on the Krylov count (5 blocks per SM by default,
+// its register budget), the projections on 4/5 of it (4 per SM).
+static void set_arnoldi_blocks(tdgl_ctx* c) {
+  c->gblocks = c->blk_stream;
+  c->nblk_orth = std::min(c->gblocks, c->blk_krylov);
+  c->nblk_arn = std::max(1, c->blk_krylov * 4 / 5);
+}
+
 // Graph variant v: 0 = finite-difference Krylov body, 1 = three-kernel Arnoldi step.
 static int ensure_graph(tdgl_ctx* c, int v) {
   if (c->gexec[v]) return TDGL_OK;
@@ -675,9 +684,7 @@ static int ensure_graph(tdgl_ctx* c, int v) {
     };
     if (!c->blk_stream) c->blk_stream = c->num_sms * env_bps("TDGL_STREAM_BLOCKS_PER_SM", 8);
     if (!c->blk_krylov) c->blk_krylov = c->num_sms * env_bps("TDGL_KRYLOV_BLOCKS_PER_SM", 5);
-    c->gblocks = c->blk_stream;
-    c->nblk_arn = c->blk_krylov;
-    c->nblk_orth = std::min(c->gblocks, c->nblk_arn);
+    set_arnoldi_blocks(c);
     const size_t tsz = c->precision == TDGL_MIXED ? sizeof(float) : sizeof(double);
     const size_t full64 = (size_t)g.ncomp * c->npf * sizeof(double);
     const size_t fullT = (size_t)g.ncomp * c->npf * tsz;
@@ -851,11 +858,7 @@ extern "C" int tdgl_ctx_set_blocks(tdgl_ctx* c, int32_t stream_blocks, int32_t k
   if (c->pending) return fail(TDGL_EINVAL, "a launch of this context has not been collected");
   c->blk_stream = stream_blocks;
   c->blk_krylov = krylov_blocks;
-  if (c->gws_ready) {
-    c->gblocks = c->blk_stream;
-    c->nblk_arn = c->blk_krylov;
-    c->nblk_orth = std::min(c->gblocks, c->nblk_arn);
-  }
+  if (c->gws_ready) set_arnoldi_blocks(c);
   for (int v = 0; v < 2; ++v) {           // rebuilt with the new shapes at the next launch
     if (c->gexec[v]) cudaGraphExecDestroy(c->gexec[v]);
     if (c->graph[v]) cudaGraphDestroy(c->graph[v]);

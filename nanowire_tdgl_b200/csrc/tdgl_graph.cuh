@@ -441,6 +441,13 @@ template <typename T> struct GGroup { static constexpr int JB = 8; };
 template <> struct GGroup<double> { static constexpr int JB = 4; };
 
 template <typename T> struct V4 { T a, b, c, d; };
+// Sum over the 32 lanes of a warp in T (butterfly: every lane gets the sum).
+template <typename T>
+__device__ __forceinline__ T warp_sum_t(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
 __device__ __forceinline__ V4<float> ld4(const float* p) {
   float4 v = *reinterpret_cast<const float4*>(p);
   return {v.x, v.y, v.z, v.w};
@@ -939,14 +946,15 @@ __device__ void arn_fold_final(const GArgs<T>& A, int ng, int ja, double* S) {
   __syncthreads();
 }
 
-// Projections <Z_ja, U_i> (i <= ja) over the interior entries (imask), in
-// passes over groups of GGroup<T>::JB vectors whose loads are all in flight
-// together.  A thread's few products per vector are summed in T (the vectors'
-// precision), warps and blocks sum in double; the last block to finish adds
-// the block partials and the orthogonalisation's ||U_ja||^2 partials in a
-// fixed order and does the column bookkeeping.
+// Projections <Z_ja, U_i> (i <= ja) over the interior entries (imask) in one
+// sweep: at each entry Z is read once and combined with the basis vectors in
+// groups of GGroup<T>::JB whose loads are all in flight together.  Each warp
+// sums its 32 products per vector in T (the vectors' precision); warps and
+// blocks accumulate in double; the partials are folded in two fixed-order
+// levels with the orthogonalisation's ||U_ja||^2 partials, and the last block
+// does the column bookkeeping.
 template <typename T>
-__global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 5 : 4) kg_arn_dots(GArgs<T> A) {
+__global__ void __launch_bounds__(kThreads, 4) kg_arn_dots(GArgs<T> A) {
   GDev* d = A.dev;
   if (!gdev_ok(d)) {
     if (blockIdx.x == 0 && threadIdx.x == 0) abort_all(A, d->status);
@@ -963,34 +971,37 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 5 : 4) kg_arn_dots(
   __syncthreads();
   constexpr int DG = GGroup<T>::JB;            // vectors per pass: their loads are all in flight at once
   const long stride = (long)gridDim.x * blockDim.x;
-  const long q0 = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  const long mo0 = (4 * q0) % npf;
-  for (int i0 = 0; i0 <= ja; i0 += DG) {
-    T acc[DG];
-#pragma unroll
-    for (int t = 0; t < DG; ++t) acc[t] = T(0);
-    long mo = mo0;
-    for (long q = q0; q < nq; q += stride) {
-      const long e = 4 * q;
-      V4<T> z = ld4(Z + e);
-      V4<T> a[DG];
-#pragma unroll
-      for (int t = 0; t < DG; ++t) a[t] = (i0 + t <= ja) ? ld4(A.UB + (long)(i0 + t) * vs + e) : V4<T>{0, 0, 0, 0};
+  // one sweep over the entries: Z is read once per entry and every vector is
+  // combined with it there; the warp adds its 32 products per vector and
+  // lane 0 accumulates the warp's sums in double (all lanes stay in the loop:
+  // its bound is warp-uniform)
+  const long wq0 = blockIdx.x * (long)blockDim.x + (threadIdx.x & ~31);
+  long mo = (4 * (wq0 + lane)) % npf;
+  for (long qb = wq0; qb < nq; qb += stride) {
+    const long q = qb + lane;
+    const bool ok = q < nq;
+    const long e = 4 * q;
+    V4<T> z = ok ? ld4(Z + e) : V4<T>{0, 0, 0, 0};
+    if (ok) {
       const uchar4 mk = *reinterpret_cast<const uchar4*>(A.imask + mo);
       if (!mk.x) z.a = T(0);
       if (!mk.y) z.b = T(0);
       if (!mk.z) z.c = T(0);
       if (!mk.w) z.d = T(0);
-#pragma unroll
-      for (int t = 0; t < DG; ++t) acc[t] += z.a * a[t].a + z.b * a[t].b + z.c * a[t].c + z.d * a[t].d;
-      mo += 4 * stride;
-      while (mo >= npf) mo -= npf;
     }
+    for (int i0 = 0; i0 <= ja; i0 += DG) {
+      V4<T> a[DG];
 #pragma unroll
-    for (int t = 0; t < DG; ++t) {
-      const double v = warp_sum((double)acc[t]);
-      if (lane == 0 && i0 + t <= ja) red[warp * nd + i0 + t] = v;
+      for (int t = 0; t < DG; ++t)
+        a[t] = (ok && i0 + t <= ja) ? ld4(A.UB + (long)(i0 + t) * vs + e) : V4<T>{0, 0, 0, 0};
+#pragma unroll
+      for (int t = 0; t < DG; ++t) {
+        const T p = warp_sum_t<T>(z.a * a[t].a + z.b * a[t].b + z.c * a[t].c + z.d * a[t].d);
+        if (lane == 0 && i0 + t <= ja) red[warp * nd + i0 + t] += (double)p;
+      }
     }
+    mo += 4 * stride;
+    while (mo >= npf) mo -= npf;
   }
   __syncthreads();
   for (int s = threadIdx.x; s <= ja; s += blockDim.x) {
