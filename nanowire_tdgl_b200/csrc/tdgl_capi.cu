@@ -122,7 +122,7 @@ struct tdgl_ctx {
   int ngroups_cap = 0;           // group-partial slots: groups of tiles or of projection blocks
   double* gpart = nullptr;
   unsigned* gticket = nullptr;
-  int apply_dots = 1;            // product and projections fused (TDGL_ARN_APPLY_DOTS=0: separate kernels)
+  int apply_dots = 0;            // product and projections in one kernel (FP64 default; TDGL_ARN_APPLY_DOTS)
   int nblk_arn = 0, nblk_orth = 0, arn_gx = 0, arn_gy = 0;
   int blk_stream = 0, blk_krylov = 0;   // blocks of the graph's grid kernels (0: defaults)
   bool pending = false, pending_noop = false;   // an uncollected tdgl_trap_launch
@@ -635,8 +635,10 @@ static int ensure_arnoldi_ws(tdgl_ctx* c) {
   c->ntiles = c->arn_gx * c->arn_gy * (g.is3d ? g.nz : 1);
   c->ngroups = (c->ntiles + 31) / 32;
   c->ngroups_cap = std::max(c->ngroups, (c->num_sms * kMaxBlocksPerSm + 31) / 32);
+  // fused product and projections: faster with FP64 vectors (the stencil's
+  // arithmetic then hides more of the basis reads), slower with FP32 ones
   const char* ead = std::getenv("TDGL_ARN_APPLY_DOTS");
-  c->apply_dots = !(ead && ead[0] == '0');
+  c->apply_dots = ead && ead[0] ? ead[0] != '0' : c->precision == TDGL_FP64;
   int rc;
   if ((rc = ctx_alloc(c, &c->UB, vb * (c->kmax + 1)))) return rc;
   if ((rc = ctx_alloc(c, &c->Zb[0], vb))) return rc;
