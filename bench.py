@@ -599,8 +599,9 @@ def run_batched(a):
                        "interior_nodes_total": sum(n_nodes), "interior_nodes_min": min(n_nodes),
                        "interior_nodes_max": max(n_nodes), "holes_total": sum(q[3] for q in desc),
                        "streams": len(bt.streams), "kmax": a.kmax},
-            "autotune_ms_per_2_steps": {str(k): v for k, v in tune.items()},
-            "shape_nodes_per_thread": bt.best,
+            "autotune_ms_per_2_steps": {f"{k[0]} nodes/thread, {'one' if k[1] else 'two'} kernel(s)": v
+                                        for k, v in tune.items()},
+            "shape": {"nodes_per_thread": bt.best[0], "fused_product_projections": bool(bt.best[1])},
             "counters": cnt,
             "max_rel_l2_psi2_batched_vs_looping": max(rel),
             "note": "batched and looping differ only in launch shapes (reduction partitions); at equal shapes "

@@ -203,11 +203,13 @@ int tdgl_trap_launch(tdgl_ctx* ctx, double* x_dev, double t, double dt_cur, int3
 int tdgl_trap_collect(tdgl_ctx* ctx, double* t, double* dt_cur, tdgl_stats* stats);
 /* Launch shape of the step graph's grid kernels: block counts, each in
  * [1, 8 x SMs], of the grid-stride passes and of the Arnoldi streams (defaults
- * 8 and 5 blocks per SM).  Any count gives a correct step; reductions are
- * deterministic for a given count.  Used by the batched form's autotuner
+ * 8 and 5 blocks per SM), and whether the Arnoldi product and projections run
+ * as one kernel (fused 1) or two (0; -1 keeps the default: one kernel for FP64
+ * vectors, two for FP32).  Any setting gives a correct step; reductions are
+ * deterministic for a given setting.  Used by the batched form's autotuner
  * (small instances run concurrently on few blocks each); the graph is rebuilt
  * at the next launch.  No reference counterpart. */
-int tdgl_ctx_set_blocks(tdgl_ctx* ctx, int32_t stream_blocks, int32_t krylov_blocks);
+int tdgl_ctx_set_blocks(tdgl_ctx* ctx, int32_t stream_blocks, int32_t krylov_blocks, int32_t fused);
 /* Forward Euler: n_steps steps of min(dt, t_stop - t) from *t (updated)
  * (src/tdgl3d/solvers/integrators.py:35-89). */
 int tdgl_euler_run(tdgl_ctx* ctx, double* x_dev, double* t, double t_stop, double dt, int32_t n_steps,

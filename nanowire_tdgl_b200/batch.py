@@ -12,9 +12,11 @@ stream with the least work so far.
 The autotuner chooses the launch shape of every instance's grid kernels: a
 candidate is a number of nodes per thread, from which each instance's block
 count follows from its size (the single-instance default of 8 blocks per SM
-for the grid-stride passes and 5 for the Arnoldi streams is one candidate).
-Each candidate is timed over a few batched steps from a snapshot of the
-states, which is restored afterwards.
+for the grid-stride passes and 5 for the Arnoldi streams is one candidate),
+and whether each Arnoldi iteration runs the product and the projections as
+one kernel or two (fewer, longer launches help small instances, whose
+kernels are launch-bound).  Each candidate is timed over a few batched steps
+from a snapshot of the states, which is restored afterwards.
 
 Each instance's arithmetic is its single-instance arithmetic (the same
 kernels, fixed-order reductions), so the results equal those of stepping the
@@ -88,7 +90,7 @@ class BatchedTrapezoidal:
                                1.0, 0.0, float(t_stop), 0, 1) for d in devices]
         self.totals = {"steps": 0, "newton_iters": 0, "krylov_iters": 0, "rejections": 0}
         self.sms = torch.cuda.get_device_properties(self.grids[0].device).multi_processor_count
-        self.shape = None                      # nodes per thread (None: single-instance default shapes)
+        self.shape = (None, -1)                # (nodes per thread or None: single-instance shapes, fused)
         self.best = None                       # the autotuner's choice
         self.set_streams(n_streams)
 
@@ -101,10 +103,13 @@ class BatchedTrapezoidal:
         self.queues, self.order = assign_streams([g.n for g in self.grids], n_streams)
         self.streams = [torch.cuda.Stream(device=self.grids[0].device) for _ in self.queues]
 
-    def set_shape(self, nodes_per_thread: Optional[int]) -> None:
+    def set_shape(self, nodes_per_thread: Optional[int], fused: int = -1) -> None:
+        """Launch shape of every instance: blocks from ``nodes_per_thread``
+        (``launch_blocks``); Arnoldi product and projections as one kernel
+        (fused 1), two (0) or the precision's default (-1)."""
         for g in self.grids:
-            g.set_blocks(*launch_blocks(g.n, nodes_per_thread, self.sms))
-        self.shape = nodes_per_thread
+            g.set_blocks(*launch_blocks(g.n, nodes_per_thread, self.sms), fused)
+        self.shape = (nodes_per_thread, fused)
 
     # -- stepping ---------------------------------------------------------------
     def _account(self, rc: int, t: float, cur: float, st: dict, i: int) -> None:
@@ -165,21 +170,22 @@ class BatchedTrapezoidal:
         torch.cuda.synchronize()
         return e0.elapsed_time(e1)
 
-    def autotune(self, candidates: Sequence = (None, 1, 2, 4, 8, 16), steps: int = 2) -> dict:
+    def autotune(self, candidates: Sequence = tuple((n, f) for n in (None, 1, 2, 4, 8) for f in (0, 1)),
+                 steps: int = 2) -> dict:
         """Time ``steps`` batched steps from the current states for each
-        nodes-per-thread candidate (None: the single-instance shapes), after
-        one untimed step that builds the graphs; keep the fastest.  States,
-        clocks and counters are restored.  Returns {candidate: ms}."""
+        (nodes per thread, fused) candidate (``set_shape``), after one untimed
+        step that builds the graphs; keep the fastest.  States, clocks and
+        counters are restored.  Returns {candidate: ms}."""
         snap = self.snapshot()
         times = {}
         for cand in candidates:
-            self.set_shape(cand)
+            self.set_shape(*cand)
             self.step(1)
             self.restore(snap)
             times[cand] = self.time_steps(steps)
             self.restore(snap)
         self.best = min(times, key=times.get)
-        self.set_shape(self.best)
+        self.set_shape(*self.best)
         return times
 
     def states(self) -> list:

@@ -123,6 +123,7 @@ struct tdgl_ctx {
   double* gpart = nullptr;
   unsigned* gticket = nullptr;
   int apply_dots = 0;            // product and projections in one kernel (FP64 default; TDGL_ARN_APPLY_DOTS)
+  int apply_dots_req = -1;       // set by tdgl_ctx_set_blocks (-1: the default)
   int nblk_arn = 0, nblk_orth = 0, arn_gx = 0, arn_gy = 0;
   int blk_stream = 0, blk_krylov = 0;   // blocks of the graph's grid kernels (0: defaults)
   bool pending = false, pending_noop = false;   // an uncollected tdgl_trap_launch
@@ -638,7 +639,8 @@ static int ensure_arnoldi_ws(tdgl_ctx* c) {
   // fused product and projections: faster with FP64 vectors (the stencil's
   // arithmetic then hides more of the basis reads), slower with FP32 ones
   const char* ead = std::getenv("TDGL_ARN_APPLY_DOTS");
-  c->apply_dots = ead && ead[0] ? ead[0] != '0' : c->precision == TDGL_FP64;
+  c->apply_dots = c->apply_dots_req >= 0 ? c->apply_dots_req
+                                         : ead && ead[0] ? ead[0] != '0' : c->precision == TDGL_FP64;
   int rc;
   if ((rc = ctx_alloc(c, &c->UB, vb * (c->kmax + 1)))) return rc;
   if ((rc = ctx_alloc(c, &c->Zb[0], vb))) return rc;
@@ -852,7 +854,7 @@ extern "C" int tdgl_trap_collect(tdgl_ctx* c, double* t, double* dt_cur, tdgl_st
   return graph_collect(c, c->pending_noop, t, dt_cur, st);
 }
 
-extern "C" int tdgl_ctx_set_blocks(tdgl_ctx* c, int32_t stream_blocks, int32_t krylov_blocks) {
+extern "C" int tdgl_ctx_set_blocks(tdgl_ctx* c, int32_t stream_blocks, int32_t krylov_blocks, int32_t fused) {
   if (!c) return fail(TDGL_EINVAL, "null argument");
   const int cap = c->num_sms * kMaxBlocksPerSm;
   if (stream_blocks < 1 || stream_blocks > cap || krylov_blocks < 1 || krylov_blocks > cap)
@@ -860,6 +862,10 @@ extern "C" int tdgl_ctx_set_blocks(tdgl_ctx* c, int32_t stream_blocks, int32_t k
   if (c->pending) return fail(TDGL_EINVAL, "a launch of this context has not been collected");
   c->blk_stream = stream_blocks;
   c->blk_krylov = krylov_blocks;
+  if (fused >= 0) {
+    c->apply_dots_req = fused ? 1 : 0;
+    if (c->UB) c->apply_dots = c->apply_dots_req;
+  }
   if (c->gws_ready) set_arnoldi_blocks(c);
   for (int v = 0; v < 2; ++v) {           // rebuilt with the new shapes at the next launch
     if (c->gexec[v]) cudaGraphExecDestroy(c->gexec[v]);

@@ -218,9 +218,11 @@ class DeviceGrid:
         rc = self.lib.tdgl_trap_collect(self.handle, C.byref(tt), C.byref(dd), C.byref(st))
         return rc, tt.value, dd.value, st.as_dict()
 
-    def set_blocks(self, stream_blocks: int, krylov_blocks: int) -> None:
-        """Block counts of the step graph's grid-stride and Arnoldi kernels."""
-        L.check(self.lib.tdgl_ctx_set_blocks(self.handle, int(stream_blocks), int(krylov_blocks)),
+    def set_blocks(self, stream_blocks: int, krylov_blocks: int, fused: int = -1) -> None:
+        """Block counts of the step graph's grid-stride and Arnoldi kernels, and
+        the Arnoldi product and projections as one kernel (1), two (0) or the
+        default (-1)."""
+        L.check(self.lib.tdgl_ctx_set_blocks(self.handle, int(stream_blocks), int(krylov_blocks), int(fused)),
                 "tdgl_ctx_set_blocks")
 
     def euler_run(self, x: torch.Tensor, t: float, t_stop: float, dt: float, n_steps: int, field: L.Field) -> float:

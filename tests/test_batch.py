@@ -53,17 +53,17 @@ def test_block_rule():
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("precision", ["mixed", "fp64"])
-@pytest.mark.parametrize("shape", [None, 2])
+@pytest.mark.parametrize("shape", [(None, -1), (2, 0), (2, 1)])
 def test_batched_equals_sequential(precision, shape):
     import nanowire_tdgl_b200 as tb
     devs, xs = _instances()
     a = tb.BatchedTrapezoidal(devs, xs, 0.1, precision=precision, kmax=96, n_streams=3)
-    a.set_shape(shape)
+    a.set_shape(*shape)
     a.step(3)
     sa = a.states()
     ta, tot_a = list(a.t), dict(a.totals)
     b = tb.BatchedTrapezoidal(devs, xs, 0.1, precision=precision, kmax=96)
-    b.set_shape(shape)
+    b.set_shape(*shape)
     b.step_sequential(3)
     for u, v in zip(sa, b.states()):
         assert np.array_equal(u, v)
@@ -83,7 +83,7 @@ def test_small_launch_shape_matches_default_within_tolerance():
     a.step(2)
     sa = a.states()
     a2 = tb.BatchedTrapezoidal(devs, xs, 0.1, **kw)
-    a2.set_shape(16)
+    a2.set_shape(16, 1)
     a2.step(2)
     for u, v in zip(sa, a2.states()):
         assert np.max(np.abs(u - v)) < 1e-9
@@ -95,13 +95,13 @@ def test_autotune_keeps_a_candidate_and_restores_states():
     devs, xs = _instances(4, seed=1)
     a = tb.BatchedTrapezoidal(devs, xs, 0.1, kmax=96)
     x_before = [x.clone() for x in a.x]
-    times = a.autotune((None, 4), steps=1)
+    times = a.autotune(((None, -1), (4, 1)), steps=1)
     assert a.best in times and a.shape == a.best
     assert all(np.array_equal(u.cpu().numpy(), v.cpu().numpy()) for u, v in zip(x_before, a.x))
     assert a.t == [0.0] * 4 and a.totals["steps"] == 0
     a.step(2)
     b = tb.BatchedTrapezoidal(devs, xs, 0.1, kmax=96)
-    b.set_shape(a.best)
+    b.set_shape(*a.best)
     b.step_sequential(2)
     for u, v in zip(a.states(), b.states()):
         assert np.array_equal(u, v)
