@@ -41,7 +41,7 @@ WORKLOAD = dict(Nx=128, Ny=128, Nz=32, h=0.5, kappa=2.0, Bz=0.5, hole=[(24, 24),
 WORKLOAD_NAME = ("trapezoidal step, 128x128x32-cell film (499,999 interior nodes), 32x32-node hole through "
                  "all planes, h=0.5, kappa=2, Bz=0.5, dt=0.1, Newton tol_f 1e-8 / tol_dx 1e-3, GCR tol 1e-6")
 HBM_FALLBACK_GBS = 6650.0
-DRAM_PER_ALG_BYTE = 0.929
+DRAM_PER_ALG_BYTE = 0.942
 
 
 def parse():
