@@ -57,9 +57,10 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget-s", type=float, default=150.0)
-    ap.add_argument("--form", choices=["precision", "adjoint", "batched"], default="precision",
+    ap.add_argument("--form", choices=["precision", "adjoint", "batched", "trilayer"], default="precision",
                     help="adjoint: gradients of the 64x64x16 differentiation workload; batched: instance-steps/s "
-                         "of 64 uneven instances stepped together against looping them (--steps per instance)")
+                         "of 64 uneven instances stepped together against looping them (--steps per instance); "
+                         "trilayer: the 256x256x64 S/I/S stack, mixed against FP64")
     ap.add_argument("--arnoldi-probe", type=int, default=None, metavar="J",
                     help="diagnostic: time the three Arnoldi-step kernels standalone at basis index J and exit")
     ap.add_argument("--kernel-timers", action="store_true",
@@ -610,8 +611,79 @@ def run_batched(a):
             "clocks": clk}
 
 
+TRI = dict(Nx=256, Ny=256, layers=(24, 16, 24), h=0.5, kappa=4.0, Bz=0.6,
+           hole=[(48, 48), (80, 48), (80, 80), (48, 80)], dt=0.1, seed=13, t_stop=200.0, kmax=160)
+
+
+def trilayer_device():
+    """256x256x64-cell superconductor / insulator / superconductor stack (24 /
+    16 / 24 cells in z, kappa 4 everywhere, psi relaxed in the insulator),
+    centred 64x64-node hole through all layers, Bz 0.6, seeded psi0 noise
+    0.01 on the superconducting nodes, phi0 = 0."""
+    import nanowire_tdgl_b200 as tb
+    w = TRI
+    b, i, t = w["layers"]
+    p = tb.SimulationParameters(Nx=w["Nx"], Ny=w["Ny"], Nz=b + i + t, hx=w["h"], hy=w["h"], hz=w["h"],
+                                kappa=w["kappa"])
+    tri = tb.Trilayer(tb.Layer(b, w["kappa"]), tb.Layer(i, w["kappa"], is_superconductor=False),
+                      tb.Layer(t, w["kappa"]))
+    dev = tb.Device(p, applied_field=tb.AppliedField(Bz=w["Bz"], t_on_fraction=1.0), trilayer=tri)
+    dev.add_hole(w["hole"])
+    rng = np.random.default_rng(w["seed"])
+    x0 = dev.initial_state()
+    n = p.n_interior
+    x0.psi[:] += 0.01 * (rng.standard_normal(n) + 1j * rng.standard_normal(n)) * dev.material.interior_sc_mask
+    return dev, x0.data.copy()
+
+
+def run_trilayer(a):
+    """Steps/s, roofline fraction and error against the FP64 stepper (the
+    reference's finite-difference product) of the mixed stepper on the large
+    trilayer, over the same K steps after W warm-up steps."""
+    import torch
+    from nanowire_tdgl_b200 import _lib as L
+    from nanowire_tdgl_b200.engine import grid_for
+    w = TRI
+    dev, x0 = trilayer_device()
+    p = dev.params
+    n_int = p.n_interior
+    runs = {}
+    for prec, jvp in (("mixed", L.TDGL_JVP_ANALYTIC), ("fp64", L.TDGL_JVP_FD)):
+        g = grid_for(p, dev.idx, dev.material, prec, w["kmax"], "gmres")
+        opts = L.TrapOpts(w["t_stop"], w["dt"], 1e-8, 1e-8, 1e-3, 1e-6, 1e-4, 20, 0, 1, jvp)
+        fld = L.Field(0.0, 0.0, w["Bz"], 1.0, 0.5, w["t_stop"], 0, 0)
+        x, ms, st = device_run(g, x0, opts, fld, a.warmup, a.steps, False)
+        runs[prec] = (g, x, ms, st)
+    (gm, xm, msm, stm), (gd, xd, msd, std) = runs["mixed"], runs["fp64"]
+    B = (0.0, 0.0, w["Bz"])
+    om, od = gm.observables(xm, B), gd.observables(xd, B)
+    def rel(k):
+        return float(torch.linalg.vector_norm(om[k] - od[k]) / torch.linalg.vector_norm(od[k]))
+    peak, peak_kind = measured_peak()
+    alg = algorithmic_bytes(n_int, "mixed", stm)
+    achieved = alg / (msm / 1e3) / 1e9
+    return {"form": "trilayer", "metric": "trapezoidal steps/s, 256x256x64 S/I/S trilayer, mixed vs FP64",
+            "value": a.steps / (msm / 1e3), "unit": "steps/s", "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": msm / a.steps, "node_updates_per_s": n_int * a.steps / (msm / 1e3),
+            "fp64_value": a.steps / (msd / 1e3), "speedup_vs_fp64": msd / msm,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind,
+                         "traffic": DRAM_PER_ALG_BYTE * alg, "algorithmic_bytes_per_launch": alg},
+            "rel_l2_vs_fp64": {"psi2": rel("psi2"), "Bz": rel("Bz"), "Jx": rel("Jx"), "Jy": rel("Jy")},
+            "max_abs_psi2_vs_fp64": float((om["psi2"] - od["psi2"]).abs().max()),
+            "dtype": "f32 Krylov / f64 state", "data": "synthetic (seeded psi0 noise)",
+            "config": {"workload": "256x256x64 cells, S/I/S 24/16/24 in z, kappa 4, Bz 0.6, centred 64x64-node "
+                                   "hole through all layers, dt 0.1, Newton tol_f 1e-8 / tol_dx 1e-3, GMRES tol "
+                                   "1e-6, kmax 160", "n_interior": n_int},
+            "counters": {k: stm[k] for k in ("newton_iters", "krylov_iters", "rejections", "max_krylov")},
+            "fp64_counters": {k: std[k] for k in ("newton_iters", "krylov_iters", "rejections", "max_krylov")}}
+
+
 def main():
     a = parse()
+    if a.form == "trilayer":
+        print(json.dumps(run_trilayer(a)), flush=True)
+        return 0
     if a.form == "adjoint":
         print(json.dumps(run_adjoint(a)), flush=True)
         return 0
