@@ -173,6 +173,23 @@ int tdgl_observables(tdgl_ctx* ctx, const double* x_dev, double Bx, double By, d
                      double* bx, double* by, double* bz, double* jx, double* jy, double* jz,
                      tdgl_stream_t stream);
 
+/* ---- analysis (post-processing of one device-layout state) ---------------- */
+/* Phase winding number of every elementary plaquette of every interior
+ * z-slice, as count_vortices_plaquette computes it for one slice
+ * (src/tdgl3d/analysis/vortex_counting.py:14-139): w_dev holds
+ * max(Nz-1, 1) x (Nx-2) x (Ny-2) doubles, index (k (Nx-2) + i) (Ny-2) + j for
+ * the plaquette with corners at interior nodes (i, j) .. (i+1, j+1) of slice
+ * k; NaN where a corner's |psi|^2 is below mask_threshold. */
+int tdgl_plaquette_winding(tdgl_ctx* ctx, const double* x_dev, double mask_threshold, double* w_dev,
+                           tdgl_stream_t stream);
+/* Mean |psi|^2 and mean |J_s| over the interior nodes with sc_ref > 0
+ * (sc_ref: interior superconducting mask in reference order, device memory;
+ * NULL: all nodes), the quantities compute_convergence_metrics compares
+ * (src/tdgl3d/analysis/convergence.py:14-117).  out_dev: 3 doubles [mean
+ * |psi|^2, mean |J_s|, node count].  Allocates its scratch on first use. */
+int tdgl_convergence_means(tdgl_ctx* ctx, const double* x_dev, const double* sc_ref_dev, double* out_dev,
+                           tdgl_stream_t stream);
+
 /* ---- solvers (device-resident control; blocking: returns after the stream work) ---- */
 
 /* Solve (I - dt/2 J(x_lin)) d = b.  Replaces tgcr_matrix_free_trap

@@ -33,3 +33,8 @@ __all__ += ["box_mean_psi2", "rhs", "trapezoidal_gradient"]
 from .batch import BatchedTrapezoidal
 
 __all__ += ["BatchedTrapezoidal"]
+from .analysis import (check_steady_state, compute_convergence_metrics, count_hole_flux_quanta,
+                       count_vortices_plaquette, count_vortices_polygon, find_vortex_cores, plaquette_windings)
+
+__all__ += ["check_steady_state", "compute_convergence_metrics", "count_hole_flux_quanta",
+            "count_vortices_plaquette", "count_vortices_polygon", "find_vortex_cores", "plaquette_windings"]

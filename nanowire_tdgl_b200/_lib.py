@@ -81,6 +81,8 @@ SIGNATURES = {
     "tdgl_newton_trap": (C.c_int, [_P, _P, _P, _D, _D, _D, _I, _D, _D, _I, _D, _D, _D, C.POINTER(Stats), _P]),
     "tdgl_trap_run": (C.c_int, [_P, _P, C.POINTER(_D), C.POINTER(_D), _I, C.POINTER(TrapOpts), C.POINTER(Field),
                                 C.POINTER(Stats), _P]),
+    "tdgl_plaquette_winding": (C.c_int, [_P, _P, _D, _P, _P]),
+    "tdgl_convergence_means": (C.c_int, [_P, _P, _P, _P, _P]),
     "tdgl_trap_launch": (C.c_int, [_P, _P, _D, _D, _I, C.POINTER(TrapOpts), C.POINTER(Field), _P]),
     "tdgl_trap_collect": (C.c_int, [_P, C.POINTER(_D), C.POINTER(_D), C.POINTER(Stats)]),
     "tdgl_ctx_set_blocks": (C.c_int, [_P, _I, _I, _I]),

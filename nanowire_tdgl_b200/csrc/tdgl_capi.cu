@@ -16,6 +16,7 @@
 #include "tdgl_stepper.cuh"
 #include "tdgl_graph.cuh"
 #include "tdgl_adjoint.cuh"
+#include "tdgl_analysis.cuh"
 
 using namespace tdgl;
 
@@ -131,6 +132,7 @@ struct tdgl_ctx {
   // adjoint scratch (allocated on first use)
   double* vjp_part = nullptr;   // 3 x vjp blocks
   double* vjp_k2 = nullptr;     // n
+  double* obs = nullptr;        // 7 x n observables scratch of tdgl_convergence_means
   std::vector<void*> owned;
   bool unsettled = false;       // initialisation memsets / copies not yet known complete
 };
@@ -384,6 +386,37 @@ extern "C" int tdgl_observables(tdgl_ctx* c, const double* x, double Bx, double 
   k_observables<<<grid_1d(c, g.n), kThreads, 0, s>>>(g, x, bterms(g, Bx, By, Bz), 1.0 / (g.hx * g.hy),
                                                       1.0 / (g.hy * g.hz), 1.0 / (g.hz * g.hx), psi2, bx, by, bz,
                                                       jx, jy, jz);
+  TDGL_CUDA(cudaGetLastError());
+  return TDGL_OK;
+}
+
+extern "C" int tdgl_plaquette_winding(tdgl_ctx* c, const double* x, double mask_threshold, double* w,
+                                      tdgl_stream_t s) {
+  if (!c || !x || !w) return fail(TDGL_EINVAL, "null argument");
+  const Grid& g = c->g;
+  const long total = (long)(g.is3d ? g.nz : 1) * (g.nx - 1) * (g.ny - 1);
+  if (total <= 0) return TDGL_OK;
+  const int blocks = (int)std::min<long>((total + kThreads - 1) / kThreads, (long)c->num_sms * 8);
+  k_plaquette<<<blocks, kThreads, 0, s>>>(g, x, mask_threshold, w);
+  TDGL_CUDA(cudaGetLastError());
+  return TDGL_OK;
+}
+
+extern "C" int tdgl_convergence_means(tdgl_ctx* c, const double* x, const double* sc_ref, double* out,
+                                      tdgl_stream_t s) {
+  if (!c || !x || !out) return fail(TDGL_EINVAL, "null argument");
+  const Grid& g = c->g;
+  const long n = g.n;
+  int rc;
+  if (!c->obs) {
+    if ((rc = ctx_alloc(c, (void**)&c->obs, sizeof(double) * 7 * (size_t)n))) return rc;
+    if ((rc = settle(c))) return rc;
+  }
+  double* o = c->obs;
+  if ((rc = tdgl_observables(c, x, 0.0, 0.0, 0.0, o, o + n, o + 2 * n, o + 3 * n, o + 4 * n, o + 5 * n, o + 6 * n,
+                             s)))
+    return rc;
+  k_conv_means<<<1, 1024, 0, s>>>(n, o, o + 4 * n, o + 5 * n, g.is3d ? o + 6 * n : nullptr, sc_ref, out);
   TDGL_CUDA(cudaGetLastError());
   return TDGL_OK;
 }

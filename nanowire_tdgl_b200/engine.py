@@ -152,6 +152,22 @@ class DeviceGrid:
                                           stream_handle()), "tdgl_observables")
         return dict(zip(("psi2", "Bx", "By", "Bz", "Jx", "Jy", "Jz"), outs))
 
+    def plaquette_winding(self, x: torch.Tensor, mask_threshold: float) -> torch.Tensor:
+        """Winding numbers of all plaquettes: (slices, Nx-2, Ny-2), NaN where masked."""
+        p = self.params
+        ns = max(p.Nz - 1, 1)
+        w = torch.empty((ns, p.Nx - 2, p.Ny - 2), dtype=torch.float64, device=self.device)
+        L.check(self.lib.tdgl_plaquette_winding(self.handle, _ptr(x), float(mask_threshold), _ptr(w),
+                                                stream_handle()), "tdgl_plaquette_winding")
+        return w
+
+    def convergence_means(self, x: torch.Tensor, sc_ref: Optional[torch.Tensor] = None) -> torch.Tensor:
+        """[mean |psi|^2, mean |J_s|, count] over nodes with sc_ref > 0 (all without)."""
+        out = torch.empty(3, dtype=torch.float64, device=self.device)
+        L.check(self.lib.tdgl_convergence_means(self.handle, _ptr(x), _ptr(sc_ref) if sc_ref is not None else None,
+                                                _ptr(out), stream_handle()), "tdgl_convergence_means")
+        return out
+
     # -- solvers --------------------------------------------------------------
     def tgcr(self, x_lin: torch.Tensor, b: torch.Tensor, dt: float, tol: float, max_iter: int, eps_mf: float,
              jvp: str, B) -> tuple[Optional[torch.Tensor], dict]:
