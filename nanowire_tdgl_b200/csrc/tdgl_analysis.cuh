@@ -52,13 +52,15 @@ __global__ void k_plaquette(Grid g, const double* __restrict__ x, double mask_th
 
 // Means over the superconducting interior nodes (sc > 0; all nodes without
 // sc) of |psi|^2 and |J_s| = sqrt(Jx^2 + Jy^2 + Jz^2), from observables in
-// reference order (src/tdgl3d/analysis/convergence.py:14-117).  One block:
+// reference order (src/tdgl3d/analysis/convergence.py:14-117).  One block of
+// exactly kThreads threads (the reduction buffer holds kWarps warps):
 // strided per-thread sums, then a fixed-order block reduction.
 // out: [mean |psi|^2, mean |J_s|, node count].
 __global__ void k_conv_means(long n, const double* __restrict__ psi2, const double* __restrict__ jx,
                              const double* __restrict__ jy, const double* __restrict__ jz,
                              const double* __restrict__ sc, double* __restrict__ out) {
   __shared__ double red[3][kWarps];
+  if (blockDim.x != kThreads) return;
   double a = 0.0, b = 0.0, c = 0.0;
   for (long r = threadIdx.x; r < n; r += blockDim.x) {
     if (sc && !(sc[r] > 0.0)) continue;

@@ -416,7 +416,7 @@ extern "C" int tdgl_convergence_means(tdgl_ctx* c, const double* x, const double
   if ((rc = tdgl_observables(c, x, 0.0, 0.0, 0.0, o, o + n, o + 2 * n, o + 3 * n, o + 4 * n, o + 5 * n, o + 6 * n,
                              s)))
     return rc;
-  k_conv_means<<<1, 1024, 0, s>>>(n, o, o + 4 * n, o + 5 * n, g.is3d ? o + 6 * n : nullptr, sc_ref, out);
+  k_conv_means<<<1, kThreads, 0, s>>>(n, o, o + 4 * n, o + 5 * n, g.is3d ? o + 6 * n : nullptr, sc_ref, out);
   TDGL_CUDA(cudaGetLastError());
   return TDGL_OK;
 }
