@@ -846,7 +846,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 5 : 3) kg_arn_orth(
 }
 
 template <typename T, bool D3>
-__global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 4 : 3) kg_arn_apply(GArgs<T> A) {
+__global__ void __launch_bounds__(kThreads, 3) kg_arn_apply(GArgs<T> A) {
   GDev* d = A.dev;
   if (!gdev_ok(d)) return;
   kt_begin(d, KT_ARN_APPLY);
@@ -1049,7 +1049,7 @@ __host__ __device__ inline size_t apply_dots_smem(int kmax) {
 }
 
 template <typename T, bool D3>
-__global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 4 : 3) kg_arn_apply_dots(GArgs<T> A) {
+__global__ void __launch_bounds__(kThreads, 3) kg_arn_apply_dots(GArgs<T> A) {
   GDev* d = A.dev;
   if (!gdev_ok(d)) {
     if (blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x == 0) abort_all(A, d->status);
