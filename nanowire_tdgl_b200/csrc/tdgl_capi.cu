@@ -129,6 +129,7 @@ struct tdgl_ctx {
   int blk_stream = 0, blk_krylov = 0;   // blocks of the graph's grid kernels (0: defaults)
   bool pending = false, pending_noop = false;   // an uncollected tdgl_trap_launch
   uint8_t* imask = nullptr;
+  uint32_t* deadmask = nullptr;   // per interior node: dead links read by the Arnoldi product
   // adjoint scratch (allocated on first use)
   double* vjp_part = nullptr;   // 3 x vjp blocks
   double* vjp_k2 = nullptr;     // n
@@ -647,6 +648,7 @@ static GArgs<T> make_gargs(tdgl_ctx* c) {
   A.arn_gx = c->arn_gx;
   A.arn_gy = c->arn_gy;
   A.apply_dots = c->apply_dots;
+  A.deadmask = c->deadmask;
   A.ntiles = c->ntiles;
   A.ngroups = c->ngroups;
   A.gpart = c->gpart;
@@ -656,6 +658,28 @@ static GArgs<T> make_gargs(tdgl_ctx* c) {
   A.cyu = c->g.kappa2 / c->g.hy2;
   A.czu = c->g.is3d ? c->g.kappa2 / c->g.hz2 : 0.0;
   return A;
+}
+
+// Dead-link masks of the interior nodes (device order), from the same rule as
+// NbM::phi; links that leave the grid (the z offsets of a 2-D grid) stay clear.
+static __global__ void k_deadmask(Grid g, uint32_t* __restrict__ mask) {
+  for (int d = blockIdx.x * blockDim.x + threadIdx.x; d < g.n; d += gridDim.x * blockDim.x) {
+    int i, j, k;
+    node_ijk(g, d, i, j, k);
+    const long m = i + (long)g.mj * j + (long)g.mk * k;
+    uint32_t w = 0u;
+#pragma unroll
+    for (int b = 0; b < 27; ++b) {
+      const int a = dead_link(b, 0), di = dead_link(b, 1), dj = dead_link(b, 2), dk = dead_link(b, 3);
+      if (!g.is3d && (a == 2 || dk != 0)) continue;
+      const long e = m + di + (long)dj * g.mj + (long)dk * g.mk;
+      const unsigned lf = g.lflags ? (unsigned)g.lflags[e] : 0u;
+      const bool dead = (a == 0 && i + di == g.Nx - 1) || (a == 1 && j + dj == g.Ny - 1) ||
+                        (a == 2 && k + dk == g.Nz - 1) || ((lf >> a) & 1u);
+      if (dead) w |= 1u << b;
+    }
+    mask[d] = w;
+  }
 }
 
 // Buffers of the three-kernel Arnoldi step (analytic products).
@@ -690,6 +714,9 @@ static int ensure_arnoldi_ws(tdgl_ctx* c) {
       for (int i = 1; i <= g.nx; ++i) im[(size_t)i + (size_t)g.mj * j + (size_t)g.mk * k] = 1;
   if ((rc = ctx_alloc(c, (void**)&c->imask, (size_t)c->npf))) return rc;
   TDGL_CUDA(cudaMemcpy(c->imask, im.data(), (size_t)c->npf, cudaMemcpyHostToDevice));
+  if ((rc = ctx_alloc(c, (void**)&c->deadmask, sizeof(uint32_t) * (size_t)g.n))) return rc;
+  k_deadmask<<<grid_1d(c, g.n), kThreads>>>(g, c->deadmask);
+  TDGL_CUDA(cudaGetLastError());
   return TDGL_OK;
 }
 

@@ -122,6 +122,7 @@ struct GArgs {
   // product and projections in one kernel (kg_arn_apply_dots): per-tile partials
   // [(kmax + 1) x ntiles] in part_arn, group partials [(kmax + 1) x ngroups]
   int apply_dots;      // 1: kg_arn_apply_dots; 0: kg_arn_apply then kg_arn_dots
+  const uint32_t* deadmask;   // per interior node: dead links among the product's neighbour reads
   int ntiles, ngroups;
   double* gpart;
   unsigned* gticket;   // [ngroups] arrival counters
@@ -792,6 +793,43 @@ struct NbM {
   }
 };
 
+// The 27 neighbour links (axis a, offset di, dj, dk) that the tangent-linear
+// stencil reads from a direction vector; bit b of a node's dead-link mask says
+// whether link dead_link(b, .) is dead (normal link on plane N-1 of its axis,
+// or a hole link), the rule NbM applies on the fly.
+__host__ __device__ constexpr int dead_link(int b, int c) {
+  constexpr int t[27][4] = {
+      {0, 0, 0, 0}, {0, -1, 0, 0}, {0, 1, 0, 0}, {0, 0, -1, 0}, {0, 0, 1, 0}, {0, -1, 1, 0}, {0, 0, 0, -1},
+      {0, 0, 0, 1}, {0, -1, 0, 1}, {1, 0, 0, 0}, {1, 0, -1, 0}, {1, -1, 0, 0}, {1, 1, 0, 0}, {1, 0, 1, 0},
+      {1, 1, -1, 0}, {1, 0, 0, -1}, {1, 0, 0, 1}, {1, 0, -1, 1}, {2, 0, 0, 0}, {2, 0, 0, -1}, {2, -1, 0, 0},
+      {2, 1, 0, 0}, {2, 0, -1, 0}, {2, 0, 1, 0}, {2, 0, 0, 1}, {2, 1, 0, -1}, {2, 0, 1, -1}};
+  return t[b][c];
+}
+
+__host__ __device__ constexpr int dead_bit(int a, int di, int dj, int dk) {
+  for (int b = 0; b < 27; ++b)
+    if (dead_link(b, 0) == a && dead_link(b, 1) == di && dead_link(b, 2) == dj && dead_link(b, 3) == dk) return b;
+  return -1;
+}
+
+// NbM with the node's precomputed dead-link mask: one load per node instead
+// of a link-flag load and plane tests per neighbour read.
+template <typename T>
+struct NbMk {
+  const T* E; long npf; long m; int mj, mk; uint32_t dm; NbM<T> slow;
+  __device__ __forceinline__ void psi(int di, int dj, int dk, T& re, T& im) const {
+    long e = m + di + (long)dj * mj + (long)dk * mk;
+    re = E[e];
+    im = E[npf + e];
+  }
+  __device__ __forceinline__ T phi(int a, int di, int dj, int dk) const {
+    const int b = dead_bit(a, di, dj, dk);
+    if (b < 0) return slow.phi(a, di, dj, dk);
+    const T v = E[(2 + a) * npf + m + di + (long)dj * mj + (long)dk * mk];
+    return ((dm >> b) & 1u) ? T(0) : v;
+  }
+};
+
 template <typename T>
 __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 5 : 3) kg_arn_orth(GArgs<T> A) {
   GDev* d = A.dev;
@@ -873,7 +911,7 @@ __global__ void __launch_bounds__(kThreads, 3) kg_arn_apply(GArgs<T> A) {
       else nc.sc = (nf & NF_SC0) ? T(0) : T(1);
     }
     NbE<T, T> X{A.XLe, npf, m, g.mj, g.mk};
-    NbM<T> P{Uj, npf, m, g.mj, g.mk, i, j, k, &g, g.lflags};
+    NbMk<T> P{Uj, npf, m, g.mj, g.mk, A.deadmask[n], NbM<T>{Uj, npf, m, g.mj, g.mk, i, j, k, &g, g.lflags}};
     T o[5];
     jvp_body<T, D3>(g, X, P, nc, nf, o);
     double z[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
@@ -1084,7 +1122,7 @@ __global__ void __launch_bounds__(kThreads, 3) kg_arn_apply_dots(GArgs<T> A) {
       else nc.sc = (nf & NF_SC0) ? T(0) : T(1);
     }
     NbE<T, T> X{A.XLe, npf, m, g.mj, g.mk};
-    NbM<T> P{Uj, npf, m, g.mj, g.mk, i, j, k, &g, g.lflags};
+    NbMk<T> P{Uj, npf, m, g.mj, g.mk, A.deadmask[n], NbM<T>{Uj, npf, m, g.mj, g.mk, i, j, k, &g, g.lflags}};
     T o[5];
     jvp_body<T, D3>(g, X, P, nc, nf, o);
     double z[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
