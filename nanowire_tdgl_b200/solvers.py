@@ -30,7 +30,9 @@ GMRES storing one vector per iteration instead of GCR's two) and ``kmax``
 
 from __future__ import annotations
 
+import ctypes
 import json
+import os
 import threading
 import time
 from concurrent.futures import ThreadPoolExecutor
@@ -269,9 +271,13 @@ class _History:
     asynchronously on a side stream into pinned host staging, and a worker
     thread copies it into row k of the output (preallocated for the expected
     number of saves; rows beyond it, after dt retries, are appended).  The
-    host-side copies overlap the next device launch, which releases the GIL
-    while it waits.
+    host copy runs as several memmove calls on a small thread pool: they
+    release the GIL (a torch CPU copy holds it, stalling the stepping thread
+    for its whole duration) and share the page faults of the fresh output
+    rows.  The host-side copies overlap the next device launch.
     """
+
+    COPY_THREADS = max(1, min(8, (os.cpu_count() or 1) // 2))
 
     def __init__(self, g, rows: int):
         self.g = g
@@ -289,6 +295,7 @@ class _History:
         self.copied = [torch.cuda.Event() for _ in range(2)]
         self.futs = [None, None]
         self.pool = ThreadPoolExecutor(max_workers=1)
+        self.copy_pool = ThreadPoolExecutor(max_workers=self.COPY_THREADS)
         self.lock = threading.Lock()
 
     def save(self, x: torch.Tensor) -> None:
@@ -305,15 +312,27 @@ class _History:
         self.futs[k] = self.pool.submit(self._land, k, self.n)
         self.n += 1
 
+    def _copy(self, dst: torch.Tensor, src: torch.Tensor) -> None:
+        nbytes = src.numel() * src.element_size()
+        per = -(-nbytes // self.COPY_THREADS)                 # ceil(nbytes / threads), rounded up to pages
+        step = (per + 4095) // 4096 * 4096 if nbytes > (1 << 20) else nbytes
+        d, s = dst.data_ptr(), src.data_ptr()
+        futs = [self.copy_pool.submit(ctypes.memmove, d + off, s + off, min(step, nbytes - off))
+                for off in range(0, nbytes, max(step, 1))]
+        for f in futs:
+            f.result()
+
     def _land(self, k: int, row: int) -> None:
         ev = self.copied[k]
         while not ev.query():
             time.sleep(5e-5)
         if row < self.rows.shape[0]:
-            self.rows[row].copy_(self.st["pin"][k])
+            self._copy(self.rows[row], self.st["pin"][k])
         else:
+            t = torch.empty_like(self.st["pin"][k], device="cpu")
+            self._copy(t, self.st["pin"][k])
             with self.lock:
-                self.extra.append((row, self.st["pin"][k].clone()))
+                self.extra.append((row, t))
 
     def result(self) -> torch.Tensor:
         """(n_saved, n_state) host tensor."""
@@ -321,6 +340,7 @@ class _History:
             if f is not None:
                 f.result()
         self.pool.shutdown(wait=True)
+        self.copy_pool.shutdown(wait=True)
         if not self.extra and self.n == self.rows.shape[0]:
             return self.rows
         more = [t for _, t in sorted(self.extra, key=lambda e: e[0])]
