@@ -198,6 +198,23 @@ class Clocks:
 # our arm
 # ---------------------------------------------------------------------------
 
+def max_over_ranks(v: float, dist: bool, device) -> float:
+    """The largest of every rank's v (the job's time is its slowest
+    replica's); v itself on one process."""
+    if not dist:
+        return float(v)
+    import torch
+    t = torch.tensor([float(v)], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(units_per_rank: float, world: int, max_ms: float) -> float:
+    """Whole-job throughput: the units all ranks processed over the slowest
+    rank's time."""
+    return world * units_per_rank / (max_ms / 1e3)
+
+
 def device_run(g, x0, opts, fld, warmup, steps, dist):
     import torch
     x = g.pack(x0)
@@ -254,11 +271,8 @@ def run_ours(a, rank, world):
     except Exception:
         pass
     clk = clocks.stop(uuid)
-    ms_t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    if dist:
-        torch.distributed.all_reduce(ms_t, op=torch.distributed.ReduceOp.MAX)
-    ms_max = float(ms_t.item())
-    value = world * a.steps / (ms_max / 1e3)
+    ms_max = max_over_ranks(ms, dist, "cuda")
+    value = job_rate(a.steps, world, ms_max)
 
     peak, peak_kind = measured_peak()
     alg = algorithmic_bytes(n_int, a.precision, st)
@@ -331,10 +345,7 @@ def run_ours(a, rank, world):
         times, hist = tb.trapezoidal(xw, p, dev.idx, sched, t_w, t_w + a.steps * w["dt"], w["dt"], **kw)
         torch.cuda.synchronize()
         el = time.perf_counter() - t0
-        el_t = torch.tensor([el], dtype=torch.float64, device="cuda")
-        if dist:
-            torch.distributed.all_reduce(el_t, op=torch.distributed.ReduceOp.MAX)
-        el = float(el_t.item())
+        el = max_over_ranks(el, dist, "cuda")
         nsteps = len(times) - 1
         sbytes = p.n_state * 16
         out["e2e"] = {"value": world * nsteps / el, "unit": "steps/s", "h2d_bytes_per_step": sbytes / nsteps,
