@@ -423,7 +423,7 @@ def arnoldi_probe(a):
     reps = max(a.steps, 1)
     res = {}
     for name, mask in (("graph", 0), ("orthogonalisation", 1), ("product", 2), ("projections", 4),
-                       ("product_and_projections", 8), ("product_two_planes", 16)):
+                       ("product_and_projections", 8)):
         L.check(g.lib.tdgl_arnoldi_probe(g.handle, j, 2, mask, stream_handle()), "tdgl_arnoldi_probe")
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)

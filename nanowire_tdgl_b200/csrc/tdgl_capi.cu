@@ -125,7 +125,6 @@ struct tdgl_ctx {
   unsigned* gticket = nullptr;
   int apply_dots = 0;            // product and projections in one kernel (FP64 default; TDGL_ARN_APPLY_DOTS)
   int apply_dots_req = -1;       // set by tdgl_ctx_set_blocks (-1: the default)
-  int apply_z2 = 0;              // 3-D product with two planes per thread (TDGL_ARN_APPLY_Z2)
   int nblk_arn = 0, nblk_orth = 0, arn_gx = 0, arn_gy = 0;
   int blk_stream = 0, blk_krylov = 0;   // blocks of the graph's grid kernels (0: defaults)
   bool pending = false, pending_noop = false;   // an uncollected tdgl_trap_launch
@@ -649,7 +648,6 @@ static GArgs<T> make_gargs(tdgl_ctx* c) {
   A.arn_gx = c->arn_gx;
   A.arn_gy = c->arn_gy;
   A.apply_dots = c->apply_dots;
-  A.apply_z2 = c->apply_z2;
   A.deadmask = c->deadmask;
   A.ntiles = c->ntiles;
   A.ngroups = c->ngroups;
@@ -697,8 +695,6 @@ static int ensure_arnoldi_ws(tdgl_ctx* c) {
   c->ngroups_cap = std::max(c->ngroups, (c->num_sms * kMaxBlocksPerSm + 31) / 32);
   // fused product and projections: faster with FP64 vectors (the stencil's
   // arithmetic then hides more of the basis reads), slower with FP32 ones
-  const char* ez2 = std::getenv("TDGL_ARN_APPLY_Z2");
-  c->apply_z2 = ez2 && ez2[0] == '1';
   const char* ead = std::getenv("TDGL_ARN_APPLY_DOTS");
   c->apply_dots = c->apply_dots_req >= 0 ? c->apply_dots_req
                                          : ead && ead[0] ? ead[0] != '0' : c->precision == TDGL_FP64;

@@ -122,7 +122,6 @@ struct GArgs {
   // product and projections in one kernel (kg_arn_apply_dots): per-tile partials
   // [(kmax + 1) x ntiles] in part_arn, group partials [(kmax + 1) x ngroups]
   int apply_dots;      // 1: kg_arn_apply_dots; 0: kg_arn_apply then kg_arn_dots
-  int apply_z2;        // 3-D product with two planes per thread (kg_arn_apply_z2)
   const uint32_t* deadmask;   // per interior node: dead links among the product's neighbour reads
   int ntiles, ngroups;
   double* gpart;
@@ -1064,63 +1063,6 @@ __global__ void __launch_bounds__(kThreads, 4) kg_arn_dots(GArgs<T> A) {
       d->kt_start[KT_ARN_DOTS] = ~0ull;
     }
   }
-}
-
-// kg_arn_apply for two consecutive planes per thread (3-D): both nodes' products
-// are formed before either is stored, so the neighbour values the two
-// stencils share (plane k+1 is the upper neighbour of the first node and the
-// centre of the second) are loaded once.
-template <typename T>
-__device__ __forceinline__ void arn_product_node(const GArgs<T>& A, const T* Uj, int i, int j, int k, T o[5]) {
-  const Grid& g = A.g;
-  const long npf = A.npf;
-  const int n = dix(g, i, j, k);
-  const long m = full_index(g, i, j, k);
-  const uint8_t nf = g.nflags[n];
-  NodeCoef<T> nc;
-  if (g.kappa_per_node) nc = node_coef<T>(g, n, nf);
-  else {
-    nc.cx = (T)A.cxu; nc.cy = (T)A.cyu; nc.cz = (T)A.czu;
-    nc.material = g.has_material != 0;
-    if (!nc.material) nc.sc = T(1);
-    else if (nf & NF_SCFRAC) nc.sc = (T)g.scint[n];
-    else nc.sc = (nf & NF_SC0) ? T(0) : T(1);
-  }
-  NbE<T, T> X{A.XLe, npf, m, g.mj, g.mk};
-  NbMk<T> P{Uj, npf, m, g.mj, g.mk, A.deadmask[n], NbM<T>{Uj, npf, m, g.mj, g.mk, i, j, k, &g, g.lflags}};
-  jvp_body<T, true>(g, X, P, nc, nf, o);
-}
-
-template <typename T>
-__global__ void __launch_bounds__(kThreads, 3) kg_arn_apply_z2(GArgs<T> A) {
-  GDev* d = A.dev;
-  if (!gdev_ok(d)) return;
-  kt_begin(d, KT_ARN_APPLY);
-  const Grid& g = A.g;
-  const int ja = d->ja;
-  const long npf = A.npf;
-  const T* Uj = A.UB + (long)ja * A.vs;
-  T* Zout = A.Zb[ja & 1];
-  const double dth = d->dta / 2.0;
-  const int i = 1 + blockIdx.x * 32 + (threadIdx.x & 31), j = 1 + blockIdx.y * 8 + (threadIdx.x >> 5);
-  const int k0 = 1 + 2 * (int)blockIdx.z;
-  if (i <= g.nx && j <= g.ny) {
-    const bool two = k0 + 1 <= g.nz;
-    T o0[5], o1[5];
-    arn_product_node<T>(A, Uj, i, j, k0, o0);
-    if (two) arn_product_node<T>(A, Uj, i, j, k0 + 1, o1);
-    const long m0 = full_index(g, i, j, k0);
-    double z[5];
-#pragma unroll
-    for (int c = 0; c < 5; ++c) z[c] = (double)Uj[c * npf + m0] - dth * (double)o0[c];
-    write_eff<T, true, true>(g, Zout, npf, i, j, k0, z, 0.0, 0.0, 0.0);
-    if (two) {
-#pragma unroll
-      for (int c = 0; c < 5; ++c) z[c] = (double)Uj[c * npf + m0 + g.mk] - dth * (double)o1[c];
-      write_eff<T, true, true>(g, Zout, npf, i, j, k0 + 1, z, 0.0, 0.0, 0.0);
-    }
-  }
-  kt_end(d, KT_ARN_APPLY);
 }
 
 // Product and projections in one kernel: each block computes Z_ja = A U_ja

@@ -92,11 +92,7 @@ cudaError_t build_trap_graph(GArgs<T> A, cudaGraph_t* out_graph, cudaGraphExec_t
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smp));
       TDGL_GCK(ck.kernel((const void*)kg_arn_apply_dots<T, D3>, tiles, kThreads, smp, A));
     } else {
-      if (D3 && A.apply_z2)
-        TDGL_GCK(ck.kernel((const void*)kg_arn_apply_z2<T>, dim3(A.arn_gx, A.arn_gy, (A.g.nz + 1) / 2), kThreads, 0,
-                           A));
-      else
-        TDGL_GCK(ck.kernel((const void*)kg_arn_apply<T, D3>, tiles, kThreads, 0, A));
+      TDGL_GCK(ck.kernel((const void*)kg_arn_apply<T, D3>, tiles, kThreads, 0, A));
       TDGL_GCK(ck.kernel((const void*)kg_arn_dots<T>, A.nblk_arn, kThreads, smd, A));
     }
   } else {

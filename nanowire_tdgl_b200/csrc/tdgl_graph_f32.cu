@@ -11,8 +11,7 @@ cudaError_t graph_build_f32(const GArgs<float>& A, cudaGraph_t* graph, cudaGraph
 
 // Diagnostic: `launches` standalone Arnoldi steps.  kernels: bit 0 the
 // orthogonalisation, bit 1 the product, bit 2 the projections, bit 3 the fused
-// product and projections, bit 4 the two-plane product; 0 = the kernels of
-// this context's graph.
+// product and projections; 0 = the kernels of this context's graph.
 cudaError_t arnoldi_probe_f32(const GArgs<float>& A, int launches, int kernels, cudaStream_t s) {
   const size_t smo = (size_t)(A.kmax + 1) * sizeof(double);
   const size_t smd = (size_t)kWarps * (A.kmax + 2) * sizeof(double);
@@ -36,8 +35,6 @@ cudaError_t arnoldi_probe_f32(const GArgs<float>& A, int launches, int kernels, 
       else kg_arn_apply<float, false><<<grid, kThreads, 0, s>>>(A);
     }
     if (kernels & 4) kg_arn_dots<float><<<A.nblk_arn, kThreads, smd, s>>>(A);
-    if ((kernels & 16) && A.g.is3d)
-      kg_arn_apply_z2<float><<<dim3(A.arn_gx, A.arn_gy, (A.g.nz + 1) / 2), kThreads, 0, s>>>(A);
     if (kernels & 8) {
       if (A.g.is3d) kg_arn_apply_dots<float, true><<<grid, kThreads, smp, s>>>(A);
       else kg_arn_apply_dots<float, false><<<grid, kThreads, smp, s>>>(A);
