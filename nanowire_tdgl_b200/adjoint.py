@@ -95,18 +95,25 @@ def rhs(xr: torch.Tensor, params, idx, material=None, B=(0.0, 0.0, 0.0)) -> torc
 
 
 def _gmres(matvec: Callable[[torch.Tensor], torch.Tensor], b: torch.Tensor, tol: float, restart: int = 60,
-           max_restarts: int = 20) -> torch.Tensor:
-    """Restarted GMRES (modified Gram-Schmidt, Givens) for A x = b, FP64."""
-    x = torch.zeros_like(b)
+           max_restarts: int = 20, x0: Optional[torch.Tensor] = None) -> torch.Tensor:
+    """Restarted GMRES for A x = b in FP64 on the device, from x0 (zero by
+    default), to ||b - A x|| <= tol ||b||.  The basis is one (restart + 1) x n
+    matrix; each iteration orthogonalises with classical Gram-Schmidt applied
+    twice (as stable as the modified form), each pass one matrix-vector
+    product for the projections and one for the update, and moves only the
+    new Hessenberg column to the host for the Givens rotations."""
+    x = torch.zeros_like(b) if x0 is None else x0.clone()
     bn = float(torch.linalg.vector_norm(b))
     if bn == 0.0:
-        return x
-    for _ in range(max_restarts):
-        r = b - matvec(x)
+        return torch.zeros_like(b)
+    n = b.numel()
+    V = torch.empty((restart + 1, n), dtype=b.dtype, device=b.device)
+    for cycle in range(max_restarts):
+        r = b.clone() if x0 is None and cycle == 0 else b - matvec(x)
         beta = float(torch.linalg.vector_norm(r))
         if beta <= tol * bn:
             return x
-        V = [r / beta]
+        V[0] = r / beta
         H = np.zeros((restart + 1, restart))
         cs, sn = np.zeros(restart), np.zeros(restart)
         gv = np.zeros(restart + 1)
@@ -114,10 +121,13 @@ def _gmres(matvec: Callable[[torch.Tensor], torch.Tensor], b: torch.Tensor, tol:
         k_done = 0
         for k in range(restart):
             w = matvec(V[k])
-            for i in range(k + 1):
-                H[i, k] = float(torch.dot(V[i], w))
-                w = w - H[i, k] * V[i]
-            H[k + 1, k] = float(torch.linalg.vector_norm(w))
+            Vk = V[:k + 1]
+            h = torch.mv(Vk, w)
+            w = w - torch.mv(Vk.t(), h)
+            h2 = torch.mv(Vk, w)
+            w = w - torch.mv(Vk.t(), h2)
+            col = torch.cat([h + h2, torch.linalg.vector_norm(w)[None]]).cpu().numpy()
+            H[:k + 2, k] = col
             for i in range(k):
                 a_, b_ = H[i, k], H[i + 1, k]
                 H[i, k] = cs[i] * a_ + sn[i] * b_
@@ -128,12 +138,11 @@ def _gmres(matvec: Callable[[torch.Tensor], torch.Tensor], b: torch.Tensor, tol:
             gv[k + 1] = -sn[k] * gv[k]
             gv[k] = cs[k] * gv[k]
             k_done = k + 1
-            if abs(gv[k + 1]) <= tol * bn or H[k, k] == 0.0:
+            if abs(gv[k + 1]) <= tol * bn or H[k, k] == 0.0 or col[-1] == 0.0:
                 break
-            V.append(w / (float(torch.linalg.vector_norm(w)) or 1.0))
+            V[k + 1] = w / float(col[-1])
         y = np.linalg.solve(np.triu(H[:k_done, :k_done]), gv[:k_done])
-        for i in range(k_done):
-            x = x + float(y[i]) * V[i]
+        x = x + torch.mv(V[:k_done].t(), torch.as_tensor(y, dtype=b.dtype, device=b.device))
     return x
 
 
@@ -200,6 +209,7 @@ def trapezoidal_gradient(x0, params, idx, t_start: float, t_stop: float, dt: flo
         return grid.vjp(xs, v, B, want_sc=want_sc)
 
     seg_starts = sorted(k for k in ckpt if k < N) if N > 0 else []
+    mu_prev = None                   # the previous step's adjoint starts the next solve
     for s0 in reversed(seg_starts):
         s1 = min(s0 + C, N)
         xs = [ckpt[s0][0].clone()]
@@ -216,7 +226,8 @@ def trapezoidal_gradient(x0, params, idx, t_start: float, t_stop: float, dt: flo
                 iters[0] += 1
                 return v - h * vjp(x_next, v)[0]
 
-            mu = _gmres(matvec, lam, adjoint_tol)
+            mu = _gmres(matvec, lam, adjoint_tol, x0=mu_prev)
+            mu_prev = mu
             gx1, gs1, _, gp1 = vjp(x_next, mu)
             gx0, gs0, _, gp0 = vjp(x_now, mu)
             lam = mu + h * gx0
