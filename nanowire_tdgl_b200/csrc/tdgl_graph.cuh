@@ -324,7 +324,7 @@ __global__ void __launch_bounds__(kThreads) kg_prepare(GArgs<T> A) {
 // Predictor: f = rhs(Xn); Xi = Xn + dt f; G = Xn + dt/2 f (integrators.py:156-158);
 // effective copies of Xi (FP64, and in T for the Jacobian products).
 template <typename T, bool D3>
-__global__ void __launch_bounds__(kThreads) kg_predict(GArgs<T> A) {
+__global__ void __launch_bounds__(kThreads, 3) kg_predict(GArgs<T> A) {
   const GDev* d = A.dev;
   if (!gdev_ok(d)) return;
   kt_begin(A.dev, KT_PREDICT);
@@ -356,7 +356,7 @@ __global__ void __launch_bounds__(kThreads) kg_predict(GArgs<T> A) {
 // Newton residual: f = rhs(Xi) into F; g = Xi - dt/2 f - G; r0 = -g into the
 // first basis vector (raw) and its effective copy.  Partials: ||r0||^2, ||x||^2, max|g|.
 template <typename T, bool D3>
-__global__ void __launch_bounds__(kThreads) kg_newton_rhs(GArgs<T> A) {
+__global__ void __launch_bounds__(kThreads, 3) kg_newton_rhs(GArgs<T> A) {
   const GDev* d = A.dev;
   if (!gdev_ok(d) || d->newton_failed) return;
   kt_begin(A.dev, KT_NRHS);
@@ -578,49 +578,6 @@ __global__ void __launch_bounds__(kThreads) kg_update(GArgs<T> A) {
   const double* cj = kry_cj(A);
   const double czxy = d->czxy, cyzx = d->cyzx, cxyz = d->cxyz;
   double acc[1] = {0.0};
-  if (A.fused) {
-    // basis on the full grid: one node per thread
-    for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < g.n; n += gridDim.x * blockDim.x) {
-      int i, j, k;
-      node_ijk(g, n, i, j, k);
-      const long m = full_index(g, i, j, k);
-      double s[NC], v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-#pragma unroll
-      for (int c = 0; c < NC; ++c) s[c] = 0.0;
-      int i0 = 0;
-      for (; i0 + 4 <= nk; i0 += 4) {
-        const T* U = A.UB + (long)i0 * A.vs + m;
-        const double c0 = cj[i0], c1 = cj[i0 + 1], c2 = cj[i0 + 2], c3 = cj[i0 + 3];
-#pragma unroll
-        for (int c = 0; c < NC; ++c) {
-          const long e = (long)c * A.npf;
-          s[c] += c0 * (double)U[e] + c1 * (double)U[A.vs + e] + c2 * (double)U[2 * A.vs + e] +
-                  c3 * (double)U[3 * A.vs + e];
-        }
-      }
-      for (; i0 < nk; ++i0) {
-        const T* U = A.UB + (long)i0 * A.vs + m;
-#pragma unroll
-        for (int c = 0; c < NC; ++c) s[c] += cj[i0] * (double)U[(long)c * A.npf];
-      }
-#pragma unroll
-      for (int c = 0; c < NC; ++c) {
-        const long e = (long)c * g.npad + n;
-        v[c] = A.Xi[e] + s[c];
-        A.Xi[e] = v[c];
-      }
-      double mm = gfinite(hypot(s[0], s[1]));
-#pragma unroll
-      for (int c = 2; c < NC; ++c) mm = fmax(mm, gfinite(fabs(s[c])));
-      acc[0] = fmax(acc[0], mm);
-      write_eff<double, D3>(g, A.Ei, A.npf, i, j, k, v, czxy, cyzx, cxyz);
-      if ((void*)A.XLe != (void*)A.Ei) write_eff<T, D3>(g, A.XLe, A.npf, i, j, k, v, czxy, cyzx, cxyz);
-    }
-    const bool mx[1] = {true};
-    block_partials<1>(acc, mx, A.part_upd, A.nblk);
-    kt_end(A.dev, KT_UPDATE);
-    return;
-  }
   const long nq = g.npad / 4;
   for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < nq; q += (long)gridDim.x * blockDim.x) {
     const long base = 4 * q;
@@ -662,6 +619,63 @@ __global__ void __launch_bounds__(kThreads) kg_update(GArgs<T> A) {
       write_eff<double, D3>(g, A.Ei, A.npf, i, j, k, v, czxy, cyzx, cxyz);
       if ((void*)A.XLe != (void*)A.Ei) write_eff<T, D3>(g, A.XLe, A.npf, i, j, k, v, czxy, cyzx, cxyz);
     }
+  }
+  const bool mx[1] = {true};
+  block_partials<1>(acc, mx, A.part_upd, A.nblk);
+  kt_end(A.dev, KT_UPDATE);
+}
+
+// Newton update of the analytic-product graph (basis on the full grid), one
+// node per thread: x += sum c_i U_i, the update's max-norm partials and the
+// effective copies.  Kept apart from kg_update so that it is not held to
+// that kernel's register budget (one block per SM).
+template <typename T, bool D3>
+__global__ void __launch_bounds__(kThreads, 3) kg_update_fused(GArgs<T> A) {
+  const GDev* d = A.dev;
+  if (!gdev_ok(d) || d->newton_failed) return;
+  kt_begin(A.dev, KT_UPDATE);
+  constexpr int NC = D3 ? 5 : 4;
+  const Grid& g = A.g;
+  const int nk = d->j;
+  const double* cj = kry_cj(A);
+  const double czxy = d->czxy, cyzx = d->cyzx, cxyz = d->cxyz;
+  double acc[1] = {0.0};
+  // basis on the full grid: one node per thread
+  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < g.n; n += gridDim.x * blockDim.x) {
+    int i, j, k;
+    node_ijk(g, n, i, j, k);
+    const long m = full_index(g, i, j, k);
+    double s[NC], v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int c = 0; c < NC; ++c) s[c] = 0.0;
+    int i0 = 0;
+    for (; i0 + 4 <= nk; i0 += 4) {
+      const T* U = A.UB + (long)i0 * A.vs + m;
+      const double c0 = cj[i0], c1 = cj[i0 + 1], c2 = cj[i0 + 2], c3 = cj[i0 + 3];
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        const long e = (long)c * A.npf;
+        s[c] += c0 * (double)U[e] + c1 * (double)U[A.vs + e] + c2 * (double)U[2 * A.vs + e] +
+                c3 * (double)U[3 * A.vs + e];
+      }
+    }
+    for (; i0 < nk; ++i0) {
+      const T* U = A.UB + (long)i0 * A.vs + m;
+#pragma unroll
+      for (int c = 0; c < NC; ++c) s[c] += cj[i0] * (double)U[(long)c * A.npf];
+    }
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      const long e = (long)c * g.npad + n;
+      v[c] = A.Xi[e] + s[c];
+      A.Xi[e] = v[c];
+    }
+    double mm = gfinite(hypot(s[0], s[1]));
+#pragma unroll
+    for (int c = 2; c < NC; ++c) mm = fmax(mm, gfinite(fabs(s[c])));
+    acc[0] = fmax(acc[0], mm);
+    write_eff<double, D3>(g, A.Ei, A.npf, i, j, k, v, czxy, cyzx, cxyz);
+    if ((void*)A.XLe != (void*)A.Ei) write_eff<T, D3>(g, A.XLe, A.npf, i, j, k, v, czxy, cyzx, cxyz);
   }
   const bool mx[1] = {true};
   block_partials<1>(acc, mx, A.part_upd, A.nblk);

@@ -75,7 +75,8 @@ cudaError_t build_trap_graph(GArgs<T> A, cudaGraph_t* out_graph, cudaGraphExec_t
   Chain cn{newton_body};
   TDGL_GCK(cn.loop(A.h_krylov, &krylov_body));
   TDGL_GCK(cn.kernel((const void*)kg_newton_solve<T>, 1, kThreads, 0, A));
-  TDGL_GCK(cn.kernel((const void*)kg_update<T, D3>, nb, kThreads, 0, A));
+  if (A.fused) TDGL_GCK(cn.kernel((const void*)kg_update_fused<T, D3>, nb, kThreads, 0, A));
+  else TDGL_GCK(cn.kernel((const void*)kg_update<T, D3>, nb, kThreads, 0, A));
   TDGL_GCK(cn.kernel((const void*)kg_newton_rhs<T, D3>, nb, kThreads, 0, A));
   TDGL_GCK(cn.kernel((const void*)kg_newton_check<T>, 1, kThreads, 0, A));
   Chain ck{krylov_body};
