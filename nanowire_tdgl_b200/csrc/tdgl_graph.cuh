@@ -508,7 +508,7 @@ __global__ void __launch_bounds__(kThreads) kg_dots(GArgs<T> A) {
 // Orthogonalisation: v~_{j+1} = W - sum_{i<j} gam_i v~_i (raw, slot j) and its
 // effective copy; partial ||v~_{j+1}||^2.  Lane work: four consecutive nodes.
 template <typename T, bool D3>
-__global__ void __launch_bounds__(kThreads, 3) kg_orth(GArgs<T> A) {
+__global__ void __launch_bounds__(kThreads) kg_orth(GArgs<T> A) {
   const GDev* d = A.dev;
   if (!gdev_ok(d)) return;
   kt_begin(A.dev, KT_ORTH);
@@ -567,7 +567,7 @@ __global__ void __launch_bounds__(kThreads, 3) kg_orth(GArgs<T> A) {
 // Newton update: x += sum_i cj_i v~_i (raw FP64), effective copies of the new
 // iterate; partial max|dx| (complex modulus on psi).
 template <typename T, bool D3>
-__global__ void __launch_bounds__(kThreads, 2) kg_update(GArgs<T> A) {
+__global__ void __launch_bounds__(kThreads) kg_update(GArgs<T> A) {
   const GDev* d = A.dev;
   if (!gdev_ok(d) || d->newton_failed) return;
   kt_begin(A.dev, KT_UPDATE);
