@@ -555,14 +555,30 @@ def batched_workload():
     return devs, xs, desc
 
 
-def run_batched(a):
+def batched_shard(sizes, rank: int, world: int) -> list:
+    """Instances of this rank: the 64 split over the ranks largest first,
+    each to the rank with the fewest interior nodes so far (independent
+    instances: no data moves between ranks)."""
+    from nanowire_tdgl_b200.batch import assign_streams
+    return sorted(assign_streams(sizes, world)[0][rank])
+
+
+def run_batched(a, rank: int = 0, world: int = 1):
     """Instance-steps/s of the 64 instances stepped together (autotuned launch
     shapes, 32 streams) against looping them one after another with the
     single-instance launch shapes; both device-timed over the same K steps per
-    instance after W warm-up steps, from the same states."""
+    instance after W warm-up steps, from the same states.  Under torchrun the
+    instances are split over the ranks and the job time is the slowest
+    rank's."""
     import torch
     import nanowire_tdgl_b200 as tb
     devs, xs, desc = batched_workload()
+    n_all = len(devs)
+    node_total = sum(d.params.n_interior for d in devs)
+    if world > 1:
+        mine = batched_shard([d.params.n_interior for d in devs], rank, world)
+        devs, xs, desc = [devs[i] for i in mine], [xs[i] for i in mine], [desc[i] for i in mine]
+    dist = world > 1
     n_nodes = [d.params.n_interior for d in devs]
     kw = dict(precision="mixed", kmax=a.kmax, newton_tol_f=1e-8, newton_tol_dx=1e-3, tol_gcr=1e-6, eps_mf=1e-4)
     bt = tb.BatchedTrapezoidal(devs, xs, BATCH["dt"], n_streams=32, **kw)
@@ -571,7 +587,9 @@ def run_batched(a):
     tune = bt.autotune(steps=2)
     bt.step(a.warmup)
     tot0 = dict(bt.totals)
-    ms_b = bt.time_steps(a.steps)
+    if dist:
+        torch.distributed.barrier()
+    ms_b = max_over_ranks(bt.time_steps(a.steps), dist, "cuda")
     cnt = {k: bt.totals[k] - tot0[k] for k in tot0}
     states_b = bt.states()
     # looping baseline: the single-instance launch shapes, one instance after another
@@ -579,13 +597,15 @@ def run_batched(a):
     lp.set_shape(None)
     lp.step_sequential(a.warmup)
     torch.cuda.synchronize()
+    if dist:
+        torch.distributed.barrier()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record()
     lp.step_sequential(a.steps)
     e1.record()
     torch.cuda.synchronize()
-    ms_l = e0.elapsed_time(e1)
+    ms_l = max_over_ranks(e0.elapsed_time(e1), dist, "cuda")
     uuid = None
     try:
         uuid = str(torch.cuda.get_device_properties(0).uuid)
@@ -598,12 +618,13 @@ def run_batched(a):
         pu, pv = np.abs(u[:n]) ** 2, np.abs(v[:n]) ** 2
         rel.append(float(np.linalg.norm(pu - pv) / np.linalg.norm(pv)))
     free, total = torch.cuda.mem_get_info()
-    inst_steps = len(devs) * a.steps
+    inst_steps = n_all * a.steps
     return {"form": "batched", "metric": "instance-steps/s, 64 seeded uneven instances, batched vs looping",
             "value": inst_steps / (ms_b / 1e3), "unit": "instance-steps/s",
             "looping_value": inst_steps / (ms_l / 1e3), "speedup_vs_looping": ms_l / ms_b,
             "steps_per_instance": a.steps, "warmup": a.warmup, "ms_batched": ms_b, "ms_looping": ms_l,
-            "node_updates_per_s": sum(n_nodes) * a.steps / (ms_b / 1e3),
+            "node_updates_per_s": node_total * a.steps / (ms_b / 1e3), "n_gpus": world,
+            "scaling": "strong" if dist else "single GPU",
             "dtype": "f32 Krylov / f64 state", "data": "synthetic (seeded instances)",
             "config": {"workload": "64 instances, Nx,Ny in {32,48,64,96}, Nz in {4,8,16}, h 0.5, kappa U[1.5,4], "
                                    "Bz U[0.1,1], 0-3 rectangular holes of side 4-16 nodes, dt 0.1, Newton tol_f "
@@ -615,7 +636,7 @@ def run_batched(a):
                                         for k, v in tune.items()},
             "shape": {"nodes_per_thread": bt.best[0], "fused_product_projections": bool(bt.best[1])},
             "counters": cnt,
-            "max_rel_l2_psi2_batched_vs_looping": max(rel),
+            "max_rel_l2_psi2_batched_vs_looping": max_over_ranks(max(rel), dist, "cuda"),
             "note": "batched and looping differ only in launch shapes (reduction partitions); at equal shapes "
                     "the results are bit-identical",
             "device_memory_in_use_gb": (total - free) / 1e9,
@@ -700,7 +721,20 @@ def main():
         return 0
     if a.form == "batched":
         os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")   # before CUDA is initialised
-        print(json.dumps(run_batched(a)), flush=True)
+        rank = int(os.environ.get("RANK", "0"))
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        if world > 1:
+            import torch
+            from datetime import timedelta
+            torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+            torch.distributed.init_process_group("nccl", timeout=timedelta(seconds=300))
+        try:
+            out = run_batched(a, rank, world)
+        finally:
+            if world > 1:
+                torch.distributed.destroy_process_group()
+        if rank == 0:
+            print(json.dumps(out), flush=True)
         return 0
     if a.arnoldi_probe is not None:
         return arnoldi_probe(a)

@@ -51,3 +51,17 @@ def test_single_process_passes_value_through():
     import bench
     assert bench.max_over_ranks(3.5, False, "cpu") == 3.5
     assert bench.job_rate(10, 1, 500.0) == pytest.approx(20.0)
+
+
+def test_batched_instances_split_over_ranks():
+    """The batched form's instances split over ranks: every instance on
+    exactly one rank, node counts balanced to within the largest instance."""
+    sys.path.insert(0, ROOT)
+    import bench
+    devs, _, _ = bench.batched_workload()
+    sizes = [d.params.n_interior for d in devs]
+    for world in (2, 4, 8):
+        shards = [bench.batched_shard(sizes, r, world) for r in range(world)]
+        assert sorted(i for s in shards for i in s) == list(range(len(sizes)))
+        loads = [sum(sizes[i] for i in s) for s in shards]
+        assert max(loads) - min(loads) <= max(sizes)
