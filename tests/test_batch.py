@@ -6,15 +6,27 @@ import numpy as np
 import pytest
 
 
-def _instances(n=5, seed=0):
+def _instances(n=5, seed=0, variety=False):
+    """Seeded instances of uneven size, kappa, field and holes; with variety,
+    the first two are a trilayer and a periodic film."""
     import nanowire_tdgl_b200 as tb
     rng = np.random.default_rng(seed)
     devs, xs = [], []
     for q in range(n):
         Nx, Ny = (int(v) for v in rng.choice([12, 16, 20, 24], 2))
         Nz = int(rng.choice([1, 4, 6]))
-        p = tb.SimulationParameters(Nx=Nx, Ny=Ny, Nz=Nz, hx=0.5, hy=0.5, hz=0.5, kappa=float(rng.uniform(1.5, 4)))
-        d = tb.Device(p, applied_field=tb.AppliedField(Bz=float(rng.uniform(0.1, 1.0)), t_on_fraction=1.0))
+        kappa = float(rng.uniform(1.5, 4))
+        field = tb.AppliedField(Bz=float(rng.uniform(0.1, 1.0)), t_on_fraction=1.0)
+        if variety and q == 0:
+            p = tb.SimulationParameters(Nx=Nx, Ny=Ny, Nz=7, hx=0.5, hy=0.5, hz=0.5, kappa=kappa)
+            tri = tb.Trilayer(tb.Layer(3, kappa), tb.Layer(2, kappa, is_superconductor=False), tb.Layer(2, kappa))
+            d = tb.Device(p, applied_field=field, trilayer=tri)
+        elif variety and q == 1:
+            p = tb.SimulationParameters(Nx=Nx, Ny=Ny, Nz=Nz, hx=0.5, hy=0.5, hz=0.5, kappa=kappa, periodic_x=True)
+            d = tb.Device(p, applied_field=field)
+        else:
+            p = tb.SimulationParameters(Nx=Nx, Ny=Ny, Nz=Nz, hx=0.5, hy=0.5, hz=0.5, kappa=kappa)
+            d = tb.Device(p, applied_field=field)
         if q % 2:
             i0, j0 = int(rng.integers(3, Nx - 8)), int(rng.integers(3, Ny - 8))
             s = int(rng.integers(3, 6))
@@ -69,6 +81,24 @@ def test_batched_equals_sequential(precision, shape):
         assert np.array_equal(u, v)
     assert ta == b.t and tot_a == b.totals
     assert all(abs(t - 0.3) < 1e-12 for t in ta)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_batched_trilayer_and_periodic_instances(precision):
+    """A trilayer (psi relaxed in the insulator) and a periodic film in the
+    batch: concurrent steps equal the one-by-one steps bit for bit."""
+    import nanowire_tdgl_b200 as tb
+    devs, xs = _instances(4, seed=3, variety=True)
+    a = tb.BatchedTrapezoidal(devs, xs, 0.1, precision=precision, kmax=96, n_streams=4)
+    a.set_shape(2, 1)
+    a.step(2)
+    b = tb.BatchedTrapezoidal(devs, xs, 0.1, precision=precision, kmax=96)
+    b.set_shape(2, 1)
+    b.step_sequential(2)
+    for u, v in zip(a.states(), b.states()):
+        assert np.array_equal(u, v)
+    assert a.totals == b.totals
 
 
 @pytest.mark.gpu
