@@ -221,8 +221,8 @@ int tdgl_trap_collect(tdgl_ctx* ctx, double* t, double* dt_cur, tdgl_stats* stat
 /* Launch shape of the step graph's grid kernels: block counts, each in
  * [1, 8 x SMs], of the grid-stride passes and of the Arnoldi streams (defaults
  * 8 and 5 blocks per SM), and whether the Arnoldi product and projections run
- * as one kernel (fused 1) or two (0; -1 keeps the default: one kernel for FP64
- * vectors, two for FP32).  Any setting gives a correct step; reductions are
+ * as one kernel (fused 1) or two (0; -1: the default, one kernel for FP64
+ * vectors and two for FP32).  Any setting gives a correct step; reductions are
  * deterministic for a given setting.  Used by the batched form's autotuner
  * (small instances run concurrently on few blocks each); the graph is rebuilt
  * at the next launch.  No reference counterpart. */

@@ -682,6 +682,16 @@ static __global__ void k_deadmask(Grid g, uint32_t* __restrict__ mask) {
   }
 }
 
+// Product and projections as one kernel or two: as set by tdgl_ctx_set_blocks,
+// else TDGL_ARN_APPLY_DOTS, else one kernel for FP64 vectors (the stencil's
+// arithmetic then hides more of the basis reads) and two for FP32 ones.
+static int apply_dots_setting(const tdgl_ctx* c) {
+  if (c->apply_dots_req >= 0) return c->apply_dots_req;
+  const char* e = std::getenv("TDGL_ARN_APPLY_DOTS");
+  if (e && e[0]) return e[0] != '0';
+  return c->precision == TDGL_FP64;
+}
+
 // Buffers of the three-kernel Arnoldi step (analytic products).
 static int ensure_arnoldi_ws(tdgl_ctx* c) {
   if (c->UB) return TDGL_OK;
@@ -693,11 +703,7 @@ static int ensure_arnoldi_ws(tdgl_ctx* c) {
   c->ntiles = c->arn_gx * c->arn_gy * (g.is3d ? g.nz : 1);
   c->ngroups = (c->ntiles + 31) / 32;
   c->ngroups_cap = std::max(c->ngroups, (c->num_sms * kMaxBlocksPerSm + 31) / 32);
-  // fused product and projections: faster with FP64 vectors (the stencil's
-  // arithmetic then hides more of the basis reads), slower with FP32 ones
-  const char* ead = std::getenv("TDGL_ARN_APPLY_DOTS");
-  c->apply_dots = c->apply_dots_req >= 0 ? c->apply_dots_req
-                                         : ead && ead[0] ? ead[0] != '0' : c->precision == TDGL_FP64;
+  c->apply_dots = apply_dots_setting(c);
   int rc;
   if ((rc = ctx_alloc(c, &c->UB, vb * (c->kmax + 1)))) return rc;
   if ((rc = ctx_alloc(c, &c->Zb[0], vb))) return rc;
@@ -922,10 +928,8 @@ extern "C" int tdgl_ctx_set_blocks(tdgl_ctx* c, int32_t stream_blocks, int32_t k
   if (c->pending) return fail(TDGL_EINVAL, "a launch of this context has not been collected");
   c->blk_stream = stream_blocks;
   c->blk_krylov = krylov_blocks;
-  if (fused >= 0) {
-    c->apply_dots_req = fused ? 1 : 0;
-    if (c->UB) c->apply_dots = c->apply_dots_req;
-  }
+  c->apply_dots_req = fused < 0 ? -1 : (fused ? 1 : 0);
+  if (c->UB) c->apply_dots = apply_dots_setting(c);
   if (c->gws_ready) set_arnoldi_blocks(c);
   for (int v = 0; v < 2; ++v) {           // rebuilt with the new shapes at the next launch
     if (c->gexec[v]) cudaGraphExecDestroy(c->gexec[v]);
