@@ -1021,58 +1021,39 @@ __global__ void __launch_bounds__(kThreads, 4) kg_arn_dots(GArgs<T> A) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int t = threadIdx.x; t < kWarps * nd; t += blockDim.x) red[t] = 0.0;
   __syncthreads();
-  // Two entries per lane and pass (q and q + stride), so that a warp sweeps
-  // the vector in half as many dependent steps; their products are added
-  // before the warp sum.
-  constexpr int DG = GGroup<T>::JB / 2;        // vectors per group, for each of the two entries
+  constexpr int DG = GGroup<T>::JB;            // vectors per pass: their loads are all in flight at once
   const long stride = (long)gridDim.x * blockDim.x;
   // one sweep over the entries: Z is read once per entry and every vector is
-  // combined with it there; the warp adds its 64 products per vector and
+  // combined with it there; the warp adds its 32 products per vector and
   // lane 0 accumulates the warp's sums in double (all lanes stay in the loop:
   // its bound is warp-uniform)
   const long wq0 = blockIdx.x * (long)blockDim.x + (threadIdx.x & ~31);
-  long mo1 = (4 * (wq0 + lane)) % npf;
-  long mo2 = (4 * (wq0 + lane + stride)) % npf;
-  const long step4 = (8 * stride) % npf;               // offset advance of two strides, reduced
-  for (long qb = wq0; qb < nq; qb += 2 * stride) {
-    const long q1 = qb + lane, q2 = q1 + stride;
-    const bool ok1 = q1 < nq, ok2 = q2 < nq;
-    const long e1 = 4 * q1, e2 = 4 * q2;
-    V4<T> z1 = ok1 ? ld4(Z + e1) : V4<T>{0, 0, 0, 0};
-    V4<T> z2 = ok2 ? ld4(Z + e2) : V4<T>{0, 0, 0, 0};
-    if (ok1) {
-      const uchar4 mk = *reinterpret_cast<const uchar4*>(A.imask + mo1);
-      if (!mk.x) z1.a = T(0);
-      if (!mk.y) z1.b = T(0);
-      if (!mk.z) z1.c = T(0);
-      if (!mk.w) z1.d = T(0);
-    }
-    if (ok2) {
-      const uchar4 mk = *reinterpret_cast<const uchar4*>(A.imask + mo2);
-      if (!mk.x) z2.a = T(0);
-      if (!mk.y) z2.b = T(0);
-      if (!mk.z) z2.c = T(0);
-      if (!mk.w) z2.d = T(0);
+  long mo = (4 * (wq0 + lane)) % npf;
+  for (long qb = wq0; qb < nq; qb += stride) {
+    const long q = qb + lane;
+    const bool ok = q < nq;
+    const long e = 4 * q;
+    V4<T> z = ok ? ld4(Z + e) : V4<T>{0, 0, 0, 0};
+    if (ok) {
+      const uchar4 mk = *reinterpret_cast<const uchar4*>(A.imask + mo);
+      if (!mk.x) z.a = T(0);
+      if (!mk.y) z.b = T(0);
+      if (!mk.z) z.c = T(0);
+      if (!mk.w) z.d = T(0);
     }
     for (int i0 = 0; i0 <= ja; i0 += DG) {
-      V4<T> a1[DG], a2[DG];
+      V4<T> a[DG];
+#pragma unroll
+      for (int t = 0; t < DG; ++t)
+        a[t] = (ok && i0 + t <= ja) ? ld4(A.UB + (long)(i0 + t) * vs + e) : V4<T>{0, 0, 0, 0};
 #pragma unroll
       for (int t = 0; t < DG; ++t) {
-        const T* U = A.UB + (long)(i0 + t) * vs;
-        a1[t] = (ok1 && i0 + t <= ja) ? ld4(U + e1) : V4<T>{0, 0, 0, 0};
-        a2[t] = (ok2 && i0 + t <= ja) ? ld4(U + e2) : V4<T>{0, 0, 0, 0};
-      }
-#pragma unroll
-      for (int t = 0; t < DG; ++t) {
-        const T p = warp_sum_t<T>(z1.a * a1[t].a + z1.b * a1[t].b + z1.c * a1[t].c + z1.d * a1[t].d +
-                                  z2.a * a2[t].a + z2.b * a2[t].b + z2.c * a2[t].c + z2.d * a2[t].d);
+        const T p = warp_sum_t<T>(z.a * a[t].a + z.b * a[t].b + z.c * a[t].c + z.d * a[t].d);
         if (lane == 0 && i0 + t <= ja) red[warp * nd + i0 + t] += (double)p;
       }
     }
-    mo1 += step4;
-    while (mo1 >= npf) mo1 -= npf;
-    mo2 += step4;
-    while (mo2 >= npf) mo2 -= npf;
+    mo += 4 * stride;
+    while (mo >= npf) mo -= npf;
   }
   __syncthreads();
   for (int s = threadIdx.x; s <= ja; s += blockDim.x) {
