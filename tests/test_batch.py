@@ -120,6 +120,27 @@ def test_small_launch_shape_matches_default_within_tolerance():
 
 
 @pytest.mark.gpu
+def test_default_shape_after_fused_shape_is_the_default():
+    """Setting the default form (fused -1) after a fused shape restores the
+    default, so a context that went through the autotuner steps like a fresh
+    one with the same shape."""
+    import nanowire_tdgl_b200 as tb
+    devs, xs = _instances(3, seed=4)
+    a = tb.BatchedTrapezoidal(devs, xs, 0.1, kmax=96)
+    a.set_shape(4, 1)
+    a.step(1)
+    a.set_shape(None, -1)
+    a.restore(([tb_x.clone() for tb_x in tb.BatchedTrapezoidal(devs, xs, 0.1, kmax=96).x], [0.0] * 3, [0.1] * 3,
+               {"steps": 0, "newton_iters": 0, "krylov_iters": 0, "rejections": 0}))
+    a.step(2)
+    b = tb.BatchedTrapezoidal(devs, xs, 0.1, kmax=96)
+    b.set_shape(None, -1)
+    b.step_sequential(2)
+    for u, v in zip(a.states(), b.states()):
+        assert np.array_equal(u, v)
+
+
+@pytest.mark.gpu
 def test_autotune_keeps_a_candidate_and_restores_states():
     import nanowire_tdgl_b200 as tb
     devs, xs = _instances(4, seed=1)
