@@ -127,11 +127,11 @@ def test_default_shape_after_fused_shape_is_the_default():
     import nanowire_tdgl_b200 as tb
     devs, xs = _instances(3, seed=4)
     a = tb.BatchedTrapezoidal(devs, xs, 0.1, kmax=96)
+    snap = a.snapshot()
     a.set_shape(4, 1)
     a.step(1)
     a.set_shape(None, -1)
-    a.restore(([tb_x.clone() for tb_x in tb.BatchedTrapezoidal(devs, xs, 0.1, kmax=96).x], [0.0] * 3, [0.1] * 3,
-               {"steps": 0, "newton_iters": 0, "krylov_iters": 0, "rejections": 0}))
+    a.restore(snap)
     a.step(2)
     b = tb.BatchedTrapezoidal(devs, xs, 0.1, kmax=96)
     b.set_shape(None, -1)
