@@ -154,6 +154,20 @@ struct NbE {
     return (T)E[(2 + a) * npf + m + di + (long)dj * mj + (long)dk * mk];
   }
 };
+// NbE through the read-only data path (ld.global.nc): for buffers that no
+// thread of the launch writes (the Arnoldi product's linearisation copy).
+template <typename T>
+struct NbEro {
+  const T* __restrict__ E; long npf; long m; int mj, mk;
+  __device__ __forceinline__ void psi(int di, int dj, int dk, T& re, T& im) const {
+    long e = m + di + (long)dj * mj + (long)dk * mk;
+    re = __ldg(E + e);
+    im = __ldg(E + npf + e);
+  }
+  __device__ __forceinline__ T phi(int a, int di, int dj, int dk) const {
+    return __ldg(E + (2 + a) * npf + m + di + (long)dj * mj + (long)dk * mk);
+  }
+};
 // E1 + s * E2 (finite-difference point x + eps v in effective form: the boundary
 // procedure is affine, so its value at x + eps v is E(x) + eps E0(v)).
 template <typename S2>
@@ -827,19 +841,20 @@ __host__ __device__ constexpr int dead_bit(int a, int di, int dj, int dk) {
 }
 
 // NbM with the node's precomputed dead-link mask: one load per node instead
-// of a link-flag load and plane tests per neighbour read.
+// of a link-flag load and plane tests per neighbour read.  The direction is
+// read-only during the product, so its loads take the read-only data path.
 template <typename T>
 struct NbMk {
-  const T* E; long npf; long m; int mj, mk; uint32_t dm; NbM<T> slow;
+  const T* __restrict__ E; long npf; long m; int mj, mk; uint32_t dm; NbM<T> slow;
   __device__ __forceinline__ void psi(int di, int dj, int dk, T& re, T& im) const {
     long e = m + di + (long)dj * mj + (long)dk * mk;
-    re = E[e];
-    im = E[npf + e];
+    re = __ldg(E + e);
+    im = __ldg(E + npf + e);
   }
   __device__ __forceinline__ T phi(int a, int di, int dj, int dk) const {
     const int b = dead_bit(a, di, dj, dk);
     if (b < 0) return slow.phi(a, di, dj, dk);
-    const T v = E[(2 + a) * npf + m + di + (long)dj * mj + (long)dk * mk];
+    const T v = __ldg(E + (2 + a) * npf + m + di + (long)dj * mj + (long)dk * mk);
     return ((dm >> b) & 1u) ? T(0) : v;
   }
 };
@@ -924,7 +939,7 @@ __global__ void __launch_bounds__(kThreads, 3) kg_arn_apply(GArgs<T> A) {
       else if (nf & NF_SCFRAC) nc.sc = (T)g.scint[n];
       else nc.sc = (nf & NF_SC0) ? T(0) : T(1);
     }
-    NbE<T, T> X{A.XLe, npf, m, g.mj, g.mk};
+    NbEro<T> X{A.XLe, npf, m, g.mj, g.mk};
     NbMk<T> P{Uj, npf, m, g.mj, g.mk, A.deadmask[n], NbM<T>{Uj, npf, m, g.mj, g.mk, i, j, k, &g, g.lflags}};
     T o[5];
     jvp_body<T, D3>(g, X, P, nc, nf, o);
@@ -1135,7 +1150,7 @@ __global__ void __launch_bounds__(kThreads, 3) kg_arn_apply_dots(GArgs<T> A) {
       else if (nf & NF_SCFRAC) nc.sc = (T)g.scint[n];
       else nc.sc = (nf & NF_SC0) ? T(0) : T(1);
     }
-    NbE<T, T> X{A.XLe, npf, m, g.mj, g.mk};
+    NbEro<T> X{A.XLe, npf, m, g.mj, g.mk};
     NbMk<T> P{Uj, npf, m, g.mj, g.mk, A.deadmask[n], NbM<T>{Uj, npf, m, g.mj, g.mk, i, j, k, &g, g.lflags}};
     T o[5];
     jvp_body<T, D3>(g, X, P, nc, nf, o);
