@@ -324,8 +324,8 @@ class _History:
 
     def _land(self, k: int, row: int) -> None:
         ev = self.copied[k]
-        while not ev.query():
-            time.sleep(5e-5)
+        while not ev.query():            # coarse polling: each wake-up takes the GIL from the stepping thread
+            time.sleep(5e-4)
         if row < self.rows.shape[0]:
             self._copy(self.rows[row], self.st["pin"][k])
         else:
