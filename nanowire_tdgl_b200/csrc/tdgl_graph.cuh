@@ -785,17 +785,6 @@ __device__ void arn_finish(const GArgs<T>& A, GDev* d, int ja, const double* S) 
   cudaGraphSetConditional(A.h_krylov, 1);
 }
 
-// Per-thread asynchronous copies global -> shared (no alignment beyond the
-// element size); each thread later reads only the slots it filled itself.
-template <typename T>
-__device__ __forceinline__ void cp_async_elem(T* dst, const T* src) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
-  if (sizeof(T) == 4) asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(src) : "memory");
-  else asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 
 // Neighbourhood of a direction vector stored raw at interior nodes: the
