@@ -6,13 +6,14 @@
 // graph with nested conditional WHILE nodes:
 //
 //   STEP while { step_begin, prepare, predict, newton_rhs, newton_init,
-//     NEWTON while { KRYLOV while { arn_orth, arn_apply },
-//                    newton_solve, update, newton_rhs, newton_check },
+//     NEWTON while { KRYLOV while { arn_orth, arn_apply, arn_dots },
+//                    newton_solve, update_fused, newton_rhs, newton_check },
 //     accept, step_end }
 //
-// with KRYLOV while { stencil, dots, fin_dots, orth, fin_orth } for
+// (arn_apply and arn_dots as one kernel, arn_apply_dots, for FP64 vectors),
+// with KRYLOV while { stencil, dots, fin_dots, orth, fin_orth } and update for
 // finite-difference Jacobian products.  Grid kernels stream over the vectors
-// and write per-block partial sums; one-block kernels (or, in arn_apply, the
+// and write per-block partial sums; one-block kernels (or, in arn_dots, the
 // last block to finish) reduce them in a fixed order
 // (repeatable sums), take every control decision on the device and set the
 // conditional handles.  No kernel waits on another block, so nothing can spin;
@@ -709,7 +710,7 @@ __global__ void __launch_bounds__(kThreads) kg_accept(GArgs<T> A) {
 }
 
 // ---------------------------------------------------------------------------
-// Two-kernel Arnoldi step (analytic Jacobian products)
+// Arnoldi step (analytic Jacobian products)
 // ---------------------------------------------------------------------------
 //
 // Step ja of a Krylov solve runs
