@@ -241,6 +241,9 @@ extern "C" int tdgl_ctx_create(const tdgl_grid_desc* gd, const tdgl_material_des
 
 extern "C" int tdgl_ctx_destroy(tdgl_ctx* c) {
   if (!c) return TDGL_OK;
+  // work of this context may still be in flight on the caller's streams (an
+  // uncollected tdgl_trap_launch): let it finish before its buffers go
+  cudaDeviceSynchronize();
   for (int v = 0; v < 2; ++v) {
     if (c->gexec[v]) cudaGraphExecDestroy(c->gexec[v]);
     if (c->graph[v]) cudaGraphDestroy(c->graph[v]);
