@@ -125,7 +125,6 @@ struct tdgl_ctx {
   unsigned* gticket = nullptr;
   int apply_dots = 0;            // product and projections in one kernel (FP64 default; TDGL_ARN_APPLY_DOTS)
   int apply_dots_req = -1;       // set by tdgl_ctx_set_blocks (-1: the default)
-  int pdl = -1;                  // programmatic edges in the Krylov body (-1: not decided; TDGL_PDL=0 disables)
   int nblk_arn = 0, nblk_orth = 0, arn_gx = 0, arn_gy = 0;
   int blk_stream = 0, blk_krylov = 0;   // blocks of the graph's grid kernels (0: defaults)
   bool pending = false, pending_noop = false;   // an uncollected tdgl_trap_launch
@@ -652,7 +651,6 @@ static GArgs<T> make_gargs(tdgl_ctx* c) {
   A.arn_gx = c->arn_gx;
   A.arn_gy = c->arn_gy;
   A.apply_dots = c->apply_dots;
-  A.pdl = c->pdl > 0;
   A.deadmask = c->deadmask;
   A.ntiles = c->ntiles;
   A.ngroups = c->ngroups;
@@ -785,28 +783,21 @@ static int ensure_graph(tdgl_ctx* c, int v) {
     c->gws_ready = true;
   }
   if (v == 1 && (rc = ensure_arnoldi_ws(c))) return rc;
-  if (c->pdl < 0) {
-    const char* ep = std::getenv("TDGL_PDL");
-    c->pdl = !(ep && ep[0] == '0');
-  }
   cudaError_t e;
-  for (;;) {
-    if (c->precision == TDGL_MIXED) {
-      GArgs<float> A = make_gargs<float>(c);
-      A.fused = v;
-      e = graph_build_f32(A, &c->graph[v], &c->gexec[v]);
-    } else {
-      GArgs<double> A = make_gargs<double>(c);
-      A.fused = v;
-      e = graph_build_f64(A, &c->graph[v], &c->gexec[v]);
-    }
-    if (e == cudaSuccess) break;
+  if (c->precision == TDGL_MIXED) {
+    GArgs<float> A = make_gargs<float>(c);
+    A.fused = v;
+    e = graph_build_f32(A, &c->graph[v], &c->gexec[v]);
+  } else {
+    GArgs<double> A = make_gargs<double>(c);
+    A.fused = v;
+    e = graph_build_f64(A, &c->graph[v], &c->gexec[v]);
+  }
+  if (e != cudaSuccess) {
     if (c->graph[v]) cudaGraphDestroy(c->graph[v]);
     c->graph[v] = nullptr;
     c->gexec[v] = nullptr;
-    if (!c->pdl) return fail(TDGL_ECUDA, std::string("building the stepper graph: ") + cudaGetErrorString(e));
-    cudaGetLastError();          // programmatic edges refused here: build with ordinary ones
-    c->pdl = 0;
+    return fail(TDGL_ECUDA, std::string("building the stepper graph: ") + cudaGetErrorString(e));
   }
   return settle(c);
 }

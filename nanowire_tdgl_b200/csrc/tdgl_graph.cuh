@@ -123,7 +123,6 @@ struct GArgs {
   // product and projections in one kernel (kg_arn_apply_dots): per-tile partials
   // [(kmax + 1) x ntiles] in part_arn, group partials [(kmax + 1) x ngroups]
   int apply_dots;      // 1: kg_arn_apply_dots; 0: kg_arn_apply then kg_arn_dots
-  int pdl;             // programmatic edges between the Arnoldi kernels of one iteration
   const uint32_t* deadmask;   // per interior node: dead links among the product's neighbour reads
   int ntiles, ngroups;
   double* gpart;
@@ -812,13 +811,6 @@ struct NbM {
   }
 };
 
-// Programmatic dependent launch: a kernel that follows a programmatic edge
-// waits here for its predecessor's completion and memory (a no-op after an
-// ordinary edge); a predecessor lets its dependents be launched once every
-// block has executed launch_dependents or exited.
-__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
-__device__ __forceinline__ void pdl_release() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
-
 // The 27 neighbour links (axis a, offset di, dj, dk) that the tangent-linear
 // stencil reads from a direction vector; bit b of a node's dead-link mask says
 // whether link dead_link(b, .) is dead (normal link on plane N-1 of its axis,
@@ -859,7 +851,6 @@ struct NbMk {
 
 template <typename T>
 __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 5 : 3) kg_arn_orth(GArgs<T> A) {
-  pdl_wait();
   GDev* d = A.dev;
   if (!gdev_ok(d)) return;
   const int ja = d->ja;
@@ -909,12 +900,10 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 5 : 3) kg_arn_orth(
   const bool mx[1] = {false};
   block_partials<1>(acc, mx, A.part_orth, A.nblk_orth);
   kt_end(d, KT_ARN_ORTH);
-  pdl_release();
 }
 
 template <typename T, bool D3>
 __global__ void __launch_bounds__(kThreads, 3) kg_arn_apply(GArgs<T> A) {
-  pdl_wait();
   GDev* d = A.dev;
   if (!gdev_ok(d)) return;
   kt_begin(d, KT_ARN_APPLY);
@@ -950,7 +939,6 @@ __global__ void __launch_bounds__(kThreads, 3) kg_arn_apply(GArgs<T> A) {
     write_eff<T, D3, true>(g, Zout, npf, i, j, k, z, 0.0, 0.0, 0.0);
   }
   kt_end(d, KT_ARN_APPLY);
-  pdl_release();
 }
 
 // Blocks of a two-level fold: groups of kTileGroup consecutive blocks.
@@ -1024,7 +1012,6 @@ __device__ void arn_fold_final(const GArgs<T>& A, int ng, int ja, double* S) {
 // does the column bookkeeping.
 template <typename T>
 __global__ void __launch_bounds__(kThreads, 4) kg_arn_dots(GArgs<T> A) {
-  pdl_wait();
   GDev* d = A.dev;
   if (!gdev_ok(d)) {
     if (blockIdx.x == 0 && threadIdx.x == 0) abort_all(A, d->status);
@@ -1120,7 +1107,6 @@ __host__ __device__ inline size_t apply_dots_smem(int kmax) {
 
 template <typename T, bool D3>
 __global__ void __launch_bounds__(kThreads, 3) kg_arn_apply_dots(GArgs<T> A) {
-  pdl_wait();
   GDev* d = A.dev;
   if (!gdev_ok(d)) {
     if (blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x == 0) abort_all(A, d->status);

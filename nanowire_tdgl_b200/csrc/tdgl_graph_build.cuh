@@ -14,12 +14,8 @@ namespace tdgl {
 struct Chain {
   cudaGraph_t g;
   cudaGraphNode_t last = nullptr;
-  // pdl: the edge from the previous kernel is programmatic, so this kernel's
-  // blocks are launched while the previous kernel's last blocks finish (it
-  // must begin with griddepcontrol.wait, and the previous kernel's blocks end
-  // with griddepcontrol.launch_dependents)
   template <class Args>
-  cudaError_t kernel(const void* fn, dim3 grid, int block, size_t smem, Args& args, bool pdl = false) {
+  cudaError_t kernel(const void* fn, dim3 grid, int block, size_t smem, Args& args) {
     cudaKernelNodeParams p{};
     p.func = const_cast<void*>(fn);
     p.gridDim = grid;
@@ -28,17 +24,7 @@ struct Chain {
     void* a[] = {&args};
     p.kernelParams = a;
     cudaGraphNode_t n;
-    cudaError_t e;
-    if (pdl && last) {
-      e = cudaGraphAddKernelNode(&n, g, nullptr, 0, &p);
-      if (e != cudaSuccess) return e;
-      cudaGraphEdgeData ed{};
-      ed.from_port = cudaGraphKernelNodePortProgrammatic;
-      ed.type = cudaGraphDependencyTypeProgrammatic;
-      e = cudaGraphAddDependencies_v2(g, &last, &n, &ed, 1);
-    } else {
-      e = cudaGraphAddKernelNode(&n, g, last ? &last : nullptr, last ? 1 : 0, &p);
-    }
+    cudaError_t e = cudaGraphAddKernelNode(&n, g, last ? &last : nullptr, last ? 1 : 0, &p);
     if (e == cudaSuccess) last = n;
     return e;
   }
@@ -105,10 +91,10 @@ cudaError_t build_trap_graph(GArgs<T> A, cudaGraph_t* out_graph, cudaGraphExec_t
       const size_t smp = apply_dots_smem<T>(A.kmax);
       TDGL_GCK(cudaFuncSetAttribute((const void*)kg_arn_apply_dots<T, D3>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smp));
-      TDGL_GCK(ck.kernel((const void*)kg_arn_apply_dots<T, D3>, tiles, kThreads, smp, A, A.pdl != 0));
+      TDGL_GCK(ck.kernel((const void*)kg_arn_apply_dots<T, D3>, tiles, kThreads, smp, A));
     } else {
-      TDGL_GCK(ck.kernel((const void*)kg_arn_apply<T, D3>, tiles, kThreads, 0, A, A.pdl != 0));
-      TDGL_GCK(ck.kernel((const void*)kg_arn_dots<T>, A.nblk_arn, kThreads, smd, A, A.pdl != 0));
+      TDGL_GCK(ck.kernel((const void*)kg_arn_apply<T, D3>, tiles, kThreads, 0, A));
+      TDGL_GCK(ck.kernel((const void*)kg_arn_dots<T>, A.nblk_arn, kThreads, smd, A));
     }
   } else {
     TDGL_GCK(ck.kernel((const void*)kg_stencil<T, D3>, nb, kThreads, 0, A));
