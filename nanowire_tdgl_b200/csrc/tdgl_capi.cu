@@ -396,10 +396,11 @@ extern "C" int tdgl_observables(tdgl_ctx* c, const double* x, double Bx, double 
 
 extern "C" int tdgl_plaquette_winding(tdgl_ctx* c, const double* x, double mask_threshold, double* w,
                                       tdgl_stream_t s) {
-  if (!c || !x || !w) return fail(TDGL_EINVAL, "null argument");
+  if (!c) return fail(TDGL_EINVAL, "null argument");
   const Grid& g = c->g;
   const long total = (long)(g.is3d ? g.nz : 1) * (g.nx - 1) * (g.ny - 1);
-  if (total <= 0) return TDGL_OK;
+  if (total <= 0) return TDGL_OK;        // no plaquettes (Nx or Ny = 2): nothing to write
+  if (!x || !w) return fail(TDGL_EINVAL, "null argument");
   const int blocks = (int)std::min<long>((total + kThreads - 1) / kThreads, (long)c->num_sms * 8);
   k_plaquette<<<blocks, kThreads, 0, s>>>(g, x, mask_threshold, w);
   TDGL_CUDA(cudaGetLastError());

@@ -168,3 +168,20 @@ def test_device_current_means_match_oracle():
         ref = orc.masked_means(S[:n, step], J, sc)[1]
         assert abs(m[key] - ref) < 1e-12 * max(1.0, abs(ref))
     assert "current_error" not in m and "current_rel_change" in m
+
+
+@pytest.mark.gpu
+def test_device_plaquettes_on_a_grid_without_plaquettes():
+    """Nx = 2: one interior column, no plaquettes; the kernel writes nothing
+    and the count is zero, as in the reference's empty scan."""
+    import nanowire_tdgl_b200 as tb
+    p = tb.SimulationParameters(Nx=2, Ny=5, Nz=3, hx=0.5, hy=0.5, hz=0.5, kappa=2.0)
+    d = tb.Device(p)
+    x = d.initial_state().data
+    sol = _sol(d, [0.0], x[:, None])
+    w = tb.plaquette_windings(sol, step=0, device=d)
+    assert w.shape == (2, 0, 3)
+    n, pos, wind = tb.count_vortices_plaquette(sol, d, slice_z=1, step=0)
+    assert n == 0 and pos.shape == (0, 2) and wind.shape == (0,)
+    m = tb.compute_convergence_metrics(sol, d, step=0, window_size=1)
+    assert m["psi2_mean_current"] == pytest.approx(1.0) and m["psi2_rel_change"] == 0.0

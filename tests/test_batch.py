@@ -156,3 +156,45 @@ def test_autotune_keeps_a_candidate_and_restores_states():
     b.step_sequential(2)
     for u, v in zip(a.states(), b.states()):
         assert np.array_equal(u, v)
+
+
+@pytest.mark.gpu
+def test_async_entry_points_reject_misuse():
+    """tdgl_trap_collect with nothing launched, a second launch before the
+    collect, and block counts outside [1, 8 x SMs] are refused with
+    TDGL_EINVAL; the context stays usable."""
+    import ctypes as C
+    import torch
+    import nanowire_tdgl_b200 as tb
+    from nanowire_tdgl_b200 import _lib as L
+    devs, xs = _instances(1, seed=5)
+    a = tb.BatchedTrapezoidal(devs, xs, 0.1, kmax=96)
+    g = a.grids[0]
+    tt, dd, st = C.c_double(0.0), C.c_double(0.0), L.Stats()
+    assert g.lib.tdgl_trap_collect(g.handle, C.byref(tt), C.byref(dd), C.byref(st)) == L.TDGL_EINVAL
+    assert g.lib.tdgl_ctx_set_blocks(g.handle, 0, 10, -1) == L.TDGL_EINVAL
+    assert g.lib.tdgl_ctx_set_blocks(g.handle, 10, 8 * a.sms + 1, -1) == L.TDGL_EINVAL
+    s = a.streams[0]
+    g.trap_launch(a.x[0], 0.0, 0.1, 1, a.opts, a.fields[0], s)
+    rc = g.lib.tdgl_trap_launch(g.handle, C.c_void_p(a.x[0].data_ptr()), 0.0, 0.1, 1, C.byref(a.opts),
+                                C.byref(a.fields[0]), C.c_void_p(s.cuda_stream))
+    assert rc == L.TDGL_EINVAL
+    assert g.lib.tdgl_ctx_set_blocks(g.handle, 10, 10, -1) == L.TDGL_EINVAL     # a launch is pending
+    s.synchronize()
+    rc, t, cur, stats = g.trap_collect()
+    assert rc == L.TDGL_OK and abs(t - 0.1) < 1e-12 and stats["steps"] == 1
+    a.t[0], a.cur[0] = t, cur
+    a.step(1)
+    assert abs(a.t[0] - 0.2) < 1e-12
+
+
+@pytest.mark.gpu
+def test_single_instance_and_more_streams_than_instances():
+    import nanowire_tdgl_b200 as tb
+    devs, xs = _instances(1, seed=6)
+    a = tb.BatchedTrapezoidal(devs, xs, 0.1, kmax=96, n_streams=8)
+    assert len(a.streams) == 1
+    a.step(2)
+    b = tb.BatchedTrapezoidal(devs, xs, 0.1, kmax=96)
+    b.step_sequential(2)
+    assert np.array_equal(a.states()[0], b.states()[0])
