@@ -565,7 +565,7 @@ def batched_shard(sizes, rank: int, world: int) -> list:
 
 def run_batched(a, rank: int = 0, world: int = 1):
     """Instance-steps/s of the 64 instances stepped together (autotuned launch
-    shapes, 32 streams) against looping them one after another with the
+    shapes, one stream per instance) against looping them one after another with the
     single-instance launch shapes; both device-timed over the same K steps per
     instance after W warm-up steps, from the same states.  Under torchrun the
     instances are split over the ranks and the job time is the slowest
@@ -581,7 +581,7 @@ def run_batched(a, rank: int = 0, world: int = 1):
     dist = world > 1
     n_nodes = [d.params.n_interior for d in devs]
     kw = dict(precision="mixed", kmax=a.kmax, newton_tol_f=1e-8, newton_tol_dx=1e-3, tol_gcr=1e-6, eps_mf=1e-4)
-    bt = tb.BatchedTrapezoidal(devs, xs, BATCH["dt"], n_streams=32, **kw)
+    bt = tb.BatchedTrapezoidal(devs, xs, BATCH["dt"], n_streams=64, **kw)
     clocks = Clocks()
     clocks.start()
     tune = bt.autotune(steps=2)
