@@ -256,3 +256,39 @@ def test_mixed_precision_stiff_kappa(tb, kappa):
     p_ref = np.abs(ref.psi(-1)) ** 2
     p_mix = np.abs(mix.psi(-1)) ** 2
     assert np.linalg.norm(p_mix - p_ref) / np.linalg.norm(p_ref) < 1e-6
+
+
+def _oracle_run(dev, x0, fld, t_stop, **kw):
+    from oracle import tdgl_oracle as orc
+    g = orc.make_grid(dev.params, dev.idx, dev.material)
+    return orc.trapezoidal(x0, g, fld, 0.0, t_stop, 0.1, **kw)
+
+
+@pytest.mark.parametrize("mode", ["ramp", "field_func"])
+def test_field_schedules_match_oracle(tb, mode):
+    """A ramped field (evaluated on the device each step) and a Python
+    field_func (evaluated on the host each step) against the oracle."""
+    from oracle import tdgl_oracle as orc
+    p = tb.SimulationParameters(Nx=10, Ny=8, Nz=4, hx=0.5, hy=0.5, hz=0.5, kappa=2.0)
+    t_stop = 0.6
+    if mode == "ramp":
+        af = tb.AppliedField(Bx=0.1, By=0.05, Bz=0.6, t_on_fraction=0.9, ramp=True, ramp_fraction=0.5)
+        fld = orc.field_schedule(Bx=0.1, By=0.05, Bz=0.6, t_on_fraction=0.9, ramp=True, ramp_fraction=0.5,
+                                 t_stop=t_stop)
+    else:
+        def ff(t, ts):
+            return 0.05 * t, 0.0, 0.4 + 0.3 * np.sin(3.0 * t / ts)
+        af = tb.AppliedField(field_func=ff)
+        fld = lambda t: ff(t, t_stop)  # noqa: E731
+    dev = tb.Device(p, applied_field=af)
+    dev.add_hole([(1.5, 1.0), (3.0, 1.0), (3.0, 2.5), (1.5, 2.5)])
+    x0 = dev.initial_state()
+    rng = np.random.default_rng(11)
+    n = x0.psi.shape[0]
+    x0.psi += 0.02 * (rng.standard_normal(n) + 1j * rng.standard_normal(n)) * dev.material.interior_sc_mask
+    kw = dict(newton_tol_f=1e-8, newton_tol_dx=1e-3, tol_gcr=1e-6)
+    sol = tb.solve(dev, t_start=0.0, t_stop=t_stop, dt=0.1, method="trapezoidal", x0=x0.data, progress=False,
+                   log_metadata=False, **kw)
+    times, hist = _oracle_run(dev, x0.data, fld, t_stop, **kw)
+    assert np.allclose(sol.times, times, rtol=0, atol=1e-14)
+    assert np.max(np.abs(sol.states - hist)) < 1e-7
