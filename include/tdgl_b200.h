@@ -214,7 +214,10 @@ int tdgl_trap_run(tdgl_ctx* ctx, double* x_dev, double* t, double* dt_cur, int32
  * steps on the stream and returns at once (GMRES contexts only; x must stay
  * valid until the stream has passed them); after the stream has completed,
  * tdgl_trap_collect returns the clock, step size, counters and status.  One
- * uncollected launch per context at a time. */
+ * uncollected launch per context at a time; while it is pending, the
+ * context's other stepping entry points (tdgl_trap_run, tdgl_newton_trap,
+ * tdgl_tgcr_trap, tdgl_euler_run, tdgl_arnoldi_probe, tdgl_ctx_set_blocks)
+ * return TDGL_EINVAL, as they share its workspace. */
 int tdgl_trap_launch(tdgl_ctx* ctx, double* x_dev, double t, double dt_cur, int32_t max_steps,
                      const tdgl_trap_opts* opts, const tdgl_field* field, tdgl_stream_t stream);
 int tdgl_trap_collect(tdgl_ctx* ctx, double* t, double* dt_cur, tdgl_stats* stats);

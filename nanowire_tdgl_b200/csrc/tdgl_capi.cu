@@ -565,6 +565,7 @@ extern "C" int tdgl_tgcr_trap(tdgl_ctx* c, const double* x_lin, const double* bv
                               double tol, int32_t max_iter, double eps_mf, int32_t jvp_mode, double Bx, double By,
                               double Bz, tdgl_stats* st, tdgl_stream_t s) {
   if (!c || !x_lin || !bvec || !dvec) return fail(TDGL_EINVAL, "null argument");
+  if (c->pending) return fail(TDGL_EINVAL, "a launch of this context has not been collected");
   if (jvp_mode == TDGL_JVP_FD && c->precision == TDGL_MIXED)
     return fail(TDGL_EINVAL, "the finite-difference product needs the FP64 context");
   int rc;
@@ -591,6 +592,7 @@ extern "C" int tdgl_newton_trap(tdgl_ctx* c, double* x, const double* gamma, dou
                                 double tol_dx, int32_t max_iter, double tol_gcr, double eps_mf, int32_t jvp_mode,
                                 double Bx, double By, double Bz, tdgl_stats* st, tdgl_stream_t s) {
   if (!c || !x || !gamma) return fail(TDGL_EINVAL, "null argument");
+  if (c->pending) return fail(TDGL_EINVAL, "a launch of this context has not been collected");
   if (jvp_mode == TDGL_JVP_FD && c->precision == TDGL_MIXED)
     return fail(TDGL_EINVAL, "the finite-difference product needs the FP64 context");
   int rc;
@@ -947,6 +949,7 @@ extern "C" int tdgl_ctx_set_blocks(tdgl_ctx* c, int32_t stream_blocks, int32_t k
 extern "C" int tdgl_trap_run(tdgl_ctx* c, double* x, double* t, double* dt_cur, int32_t max_steps,
                              const tdgl_trap_opts* o, const tdgl_field* f, tdgl_stats* st, tdgl_stream_t s) {
   if (!c || !x || !t || !dt_cur || !o || !f) return fail(TDGL_EINVAL, "null argument");
+  if (c->pending) return fail(TDGL_EINVAL, "a launch of this context has not been collected");
   if (o->jvp_mode == TDGL_JVP_FD && c->precision == TDGL_MIXED)
     return fail(TDGL_EINVAL, "the finite-difference product needs the FP64 context");
   if (c->krylov == KRY_GMRES) return run_graph(c, x, t, dt_cur, max_steps, o, f, st, s);
@@ -1001,6 +1004,7 @@ static void host_field(const tdgl_field* f, double t, double& bx, double& by, do
 extern "C" int tdgl_euler_run(tdgl_ctx* c, double* x, double* t, double t_stop, double dt, int32_t n_steps,
                               const tdgl_field* f, tdgl_stream_t s) {
   if (!c || !x || !t || !f) return fail(TDGL_EINVAL, "null argument");
+  if (c->pending) return fail(TDGL_EINVAL, "a launch of this context has not been collected");
   double* a = x;
   double* b = c->s_x;
   for (int i = 0; i < n_steps; ++i) {
@@ -1018,6 +1022,7 @@ extern "C" int tdgl_euler_run(tdgl_ctx* c, double* x, double* t, double t_stop, 
 
 extern "C" int tdgl_arnoldi_probe(tdgl_ctx* c, int32_t ja, int32_t launches, int32_t kernels, tdgl_stream_t s) {
   if (!c || launches < 0) return fail(TDGL_EINVAL, "invalid argument");
+  if (c->pending) return fail(TDGL_EINVAL, "a launch of this context has not been collected");
   int rc;
   if ((rc = ensure_graph(c, 1))) return rc;
   if (ja < 0 || ja > c->kmax) return fail(TDGL_EINVAL, "ja must lie in [0, kmax]");

@@ -180,6 +180,10 @@ def test_async_entry_points_reject_misuse():
                                 C.byref(a.fields[0]), C.c_void_p(s.cuda_stream))
     assert rc == L.TDGL_EINVAL
     assert g.lib.tdgl_ctx_set_blocks(g.handle, 10, 10, -1) == L.TDGL_EINVAL     # a launch is pending
+    rc = g.lib.tdgl_trap_run(g.handle, C.c_void_p(a.x[0].data_ptr()), C.byref(C.c_double(0.0)),
+                             C.byref(C.c_double(0.1)), 1, C.byref(a.opts), C.byref(a.fields[0]), C.byref(L.Stats()),
+                             C.c_void_p(s.cuda_stream))
+    assert rc == L.TDGL_EINVAL                                                    # shares the workspace
     s.synchronize()
     rc, t, cur, stats = g.trap_collect()
     assert rc == L.TDGL_OK and abs(t - 0.1) < 1e-12 and stats["steps"] == 1
