@@ -733,12 +733,12 @@ static int ensure_arnoldi_ws(tdgl_ctx* c) {
 }
 
 // Block counts of the graph's grid kernels from the stream and Krylov settings:
-// the orthogonalisation runs on the Krylov count (5 blocks per SM by default,
-// its register budget), the projections on 4/5 of it (4 per SM).
+// the orthogonalisation and the projections run on 4/5 of the Krylov count
+// (4 blocks per SM by default, their register budgets).
 static void set_arnoldi_blocks(tdgl_ctx* c) {
   c->gblocks = c->blk_stream;
-  c->nblk_orth = std::min(c->gblocks, c->blk_krylov);
   c->nblk_arn = std::max(1, c->blk_krylov * 4 / 5);
+  c->nblk_orth = std::min(c->gblocks, c->nblk_arn);
 }
 
 // Graph variant v: 0 = finite-difference Krylov body, 1 = three-kernel Arnoldi step.

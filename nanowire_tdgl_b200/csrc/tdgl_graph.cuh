@@ -850,7 +850,7 @@ struct NbMk {
 };
 
 template <typename T>
-__global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 5 : 3) kg_arn_orth(GArgs<T> A) {
+__global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 4 : 3) kg_arn_orth(GArgs<T> A) {
   GDev* d = A.dev;
   if (!gdev_ok(d)) return;
   const int ja = d->ja;
@@ -873,6 +873,19 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 5 : 3) kg_arn_orth(
     double v[4] = {sc * (double)z.a, sc * (double)z.b, sc * (double)z.c, sc * (double)z.d};
     const T* U = A.UB + e;
     int i = 0;
+    for (; i + 8 <= ja; i += 8) {                // eight vectors' loads in flight together
+      V4<T> a[8];
+#pragma unroll
+      for (int t = 0; t < 8; ++t) a[t] = ld4(U + (long)(i + t) * vs);
+#pragma unroll
+      for (int t = 0; t < 8; ++t) {
+        const double gt = gsm[i + t];
+        v[0] -= gt * (double)a[t].a;
+        v[1] -= gt * (double)a[t].b;
+        v[2] -= gt * (double)a[t].c;
+        v[3] -= gt * (double)a[t].d;
+      }
+    }
     for (; i + 4 <= ja; i += 4) {
       const V4<T> a0 = ld4(U + (long)i * vs), a1 = ld4(U + (long)(i + 1) * vs);
       const V4<T> a2 = ld4(U + (long)(i + 2) * vs), a3 = ld4(U + (long)(i + 3) * vs);
