@@ -1066,8 +1066,9 @@ __global__ void __launch_bounds__(kThreads, 4) kg_arn_dots(GArgs<T> A) {
         a[t] = (ok && i0 + t <= ja) ? ld4(A.UB + (long)(i0 + t) * vs + e) : V4<T>{0, 0, 0, 0};
 #pragma unroll
       for (int t = 0; t < DG; ++t) {
+        if (i0 + t > ja) break;                  // warp-uniform: no sums for vectors past ja
         const T p = warp_sum_t<T>(z.a * a[t].a + z.b * a[t].b + z.c * a[t].c + z.d * a[t].d);
-        if (lane == 0 && i0 + t <= ja) red[warp * nd + i0 + t] += (double)p;
+        if (lane == 0) red[warp * nd + i0 + t] += (double)p;
       }
     }
     mo += 4 * stride;
