@@ -20,8 +20,6 @@ intended current metrics on the device instead), and
 
 from __future__ import annotations
 
-from typing import Optional
-
 import numpy as np
 import torch
 

@@ -21,7 +21,7 @@ from __future__ import annotations
 
 import copy as _copy
 from dataclasses import dataclass, field
-from typing import Optional, Sequence
+from typing import Sequence
 
 import numpy as np
 from numpy.typing import NDArray
