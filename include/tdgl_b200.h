@@ -209,6 +209,15 @@ int tdgl_newton_trap(tdgl_ctx* ctx, double* x_dev, const double* gamma_dev, doub
  * loop of trapezoidal (src/tdgl3d/solvers/integrators.py:150-197). */
 int tdgl_trap_run(tdgl_ctx* ctx, double* x_dev, double* t, double* dt_cur, int32_t max_steps,
                   const tdgl_trap_opts* opts, const tdgl_field* field, tdgl_stats* stats, tdgl_stream_t stream);
+/* Adjoint trapezoidal solve (no reference counterpart): (I - h J(x)^T) mu = b
+ * for the RHS with field (Bx, By, Bz), J^T applied by the adjoint kernel of
+ * tdgl_vjp, by GMRES from mu = 0 to ||b - A mu|| <= tol ||b||, entirely on
+ * the device (one graph launch; the host reads the outcome once).  FP64
+ * contexts only; x, b, mu in the device layout.  Stops at kmax iterations
+ * without restart: TDGL_ENOCONV then, with the last iterate in mu (a caller
+ * can restart from it).  *iters = iterations.  Synchronises the stream. */
+int tdgl_adjoint_solve(tdgl_ctx* ctx, const double* x_dev, const double* b_dev, double* mu_dev, double h,
+                       double tol, double Bx, double By, double Bz, int32_t* iters, tdgl_stream_t stream);
 /* tdgl_trap_run in two halves, for stepping many contexts concurrently (the
  * batched form; no reference counterpart): tdgl_trap_launch enqueues the
  * steps on the stream and returns at once (GMRES contexts only; x must stay

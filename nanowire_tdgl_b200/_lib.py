@@ -83,6 +83,7 @@ SIGNATURES = {
                                 C.POINTER(Stats), _P]),
     "tdgl_plaquette_winding": (C.c_int, [_P, _P, _D, _P, _P]),
     "tdgl_convergence_means": (C.c_int, [_P, _P, _P, _P, _P]),
+    "tdgl_adjoint_solve": (C.c_int, [_P, _P, _P, _P, _D, _D, _D, _D, _D, C.POINTER(_I), _P]),
     "tdgl_trap_launch": (C.c_int, [_P, _P, _D, _D, _I, C.POINTER(TrapOpts), C.POINTER(Field), _P]),
     "tdgl_trap_collect": (C.c_int, [_P, C.POINTER(_D), C.POINTER(_D), C.POINTER(Stats)]),
     "tdgl_ctx_set_blocks": (C.c_int, [_P, _I, _I, _I]),

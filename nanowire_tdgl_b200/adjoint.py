@@ -208,8 +208,12 @@ def trapezoidal_gradient(x0, params, idx, t_start: float, t_stop: float, dt: flo
     def vjp(xs, v):
         return grid.vjp(xs, v, B, want_sc=want_sc)
 
+    # the transposed step systems are solved on the device (one graph per
+    # solve, FP64 context); a solve that reaches kmax without converging is
+    # restarted on the host from its last iterate
+    adj_grid = grid_for(params, idx, material, "fp64", kmax)
+
     seg_starts = sorted(k for k in ckpt if k < N) if N > 0 else []
-    mu_prev = None                   # the previous step's adjoint starts the next solve
     for s0 in reversed(seg_starts):
         s1 = min(s0 + C, N)
         xs = [ckpt[s0][0].clone()]
@@ -226,8 +230,10 @@ def trapezoidal_gradient(x0, params, idx, t_start: float, t_stop: float, dt: flo
                 iters[0] += 1
                 return v - h * vjp(x_next, v)[0]
 
-            mu = _gmres(matvec, lam, adjoint_tol, x0=mu_prev)
-            mu_prev = mu
+            mu, it, ok = adj_grid.adjoint_solve(x_next, lam, h, adjoint_tol, B)
+            iters[0] += it
+            if not ok:
+                mu = _gmres(matvec, lam, adjoint_tol, x0=mu)
             gx1, gs1, _, gp1 = vjp(x_next, mu)
             gx0, gs0, _, gp0 = vjp(x_now, mu)
             lam = mu + h * gx0

@@ -17,6 +17,7 @@
 #include "tdgl_graph.cuh"
 #include "tdgl_adjoint.cuh"
 #include "tdgl_analysis.cuh"
+#include "tdgl_adjoint_graph.cuh"
 
 using namespace tdgl;
 
@@ -134,6 +135,10 @@ struct tdgl_ctx {
   double* vjp_part = nullptr;   // 3 x vjp blocks
   double* vjp_k2 = nullptr;     // n
   double* obs = nullptr;        // 7 x n observables scratch of tdgl_convergence_means
+  // device-resident adjoint solve (tdgl_adjoint_solve): x, b, mu, T (L each) and its graph
+  double* adj = nullptr;
+  cudaGraph_t adj_graph = nullptr;
+  cudaGraphExec_t adj_exec = nullptr;
   std::vector<void*> owned;
   bool unsettled = false;       // initialisation memsets / copies not yet known complete
 };
@@ -248,6 +253,8 @@ extern "C" int tdgl_ctx_destroy(tdgl_ctx* c) {
     if (c->gexec[v]) cudaGraphExecDestroy(c->gexec[v]);
     if (c->graph[v]) cudaGraphDestroy(c->graph[v]);
   }
+  if (c->adj_exec) cudaGraphExecDestroy(c->adj_exec);
+  if (c->adj_graph) cudaGraphDestroy(c->adj_graph);
   for (void* p : c->owned) cudaFree(p);
   if (c->ctl_host) cudaFreeHost(c->ctl_host);
   if (c->gdev_host) cudaFreeHost(c->gdev_host);
@@ -905,6 +912,53 @@ static int run_graph(tdgl_ctx* c, double* x, double* t, double* dt_cur, int32_t 
   if (rc) return rc;
   if (!noop) TDGL_CUDA(cudaStreamSynchronize(s));
   return graph_collect(c, noop, t, dt_cur, st);
+}
+
+extern "C" int tdgl_adjoint_solve(tdgl_ctx* c, const double* x, const double* b, double* mu, double h, double tol,
+                                  double Bx, double By, double Bz, int32_t* iters, tdgl_stream_t s) {
+  if (!c || !x || !b || !mu) return fail(TDGL_EINVAL, "null argument");
+  if (c->pending) return fail(TDGL_EINVAL, "a launch of this context has not been collected");
+  if (c->precision != TDGL_FP64) return fail(TDGL_EINVAL, "the adjoint solve needs an FP64 context");
+  int rc;
+  if ((rc = ensure_graph(c, 0))) return rc;            // the stepper workspace the solve shares
+  const size_t L = (size_t)c->L;
+  if (!c->adj) {
+    if ((rc = ctx_alloc(c, (void**)&c->adj, sizeof(double) * 4 * L))) return rc;
+    if ((rc = settle(c))) return rc;
+  }
+  if (!c->adj_exec) {
+    GArgs<double> A = make_gargs<double>(c);
+    A.ax = c->adj;
+    A.ab = c->adj + L;
+    A.amu = c->adj + 2 * L;
+    A.aT = c->adj + 3 * L;
+    cudaError_t e = c->g.is3d ? build_adjoint_graph<true>(A, &c->adj_graph, &c->adj_exec)
+                              : build_adjoint_graph<false>(A, &c->adj_graph, &c->adj_exec);
+    if (e != cudaSuccess) {
+      if (c->adj_graph) cudaGraphDestroy(c->adj_graph);
+      c->adj_graph = nullptr;
+      c->adj_exec = nullptr;
+      return fail(TDGL_ECUDA, std::string("building the adjoint graph: ") + cudaGetErrorString(e));
+    }
+  }
+  GDev& hd = *c->gdev_host;
+  std::memset(&hd, 0, sizeof(GDev));
+  hd.dta = 2.0 * h;
+  hd.tol_gcr = tol;
+  hd.krylov_max_iter = c->kmax;
+  hd.watchdog_cap = (long long)c->kmax + 100;
+  hd.Bx = Bx; hd.By = By; hd.Bz = Bz;
+  for (int k = 0; k < kKTypes; ++k) hd.kt_start[k] = ~0ull;
+  TDGL_CUDA(cudaMemcpyAsync(c->adj, x, L * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  TDGL_CUDA(cudaMemcpyAsync(c->adj + L, b, L * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  TDGL_CUDA(cudaMemcpyAsync(c->gdev, &hd, sizeof(GDev), cudaMemcpyHostToDevice, s));
+  TDGL_CUDA(cudaGraphLaunch(c->adj_exec, s));
+  TDGL_CUDA(cudaMemcpyAsync(&hd, c->gdev, sizeof(GDev), cudaMemcpyDeviceToHost, s));
+  TDGL_CUDA(cudaMemcpyAsync(mu, c->adj + 2 * L, L * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  TDGL_CUDA(cudaStreamSynchronize(s));
+  if (iters) *iters = hd.j;
+  if (hd.status != GS_OK) return graph_status(hd.status);
+  return hd.accepted ? TDGL_OK : TDGL_ENOCONV;
 }
 
 extern "C" int tdgl_trap_launch(tdgl_ctx* c, double* x, double t, double dt_cur, int32_t max_steps,

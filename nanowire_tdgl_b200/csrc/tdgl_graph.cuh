@@ -124,6 +124,12 @@ struct GArgs {
   // [(kmax + 1) x ntiles] in part_arn, group partials [(kmax + 1) x ngroups]
   int apply_dots;      // 1: kg_arn_apply_dots; 0: kg_arn_apply then kg_arn_dots
   const uint32_t* deadmask;   // per interior node: dead links among the product's neighbour reads
+  // adjoint solve (tdgl_adjoint_graph.cuh): linearisation state, right-hand
+  // side, solution, J^T v scratch (device layout, L entries each)
+  const double* ax;
+  const double* ab;
+  double* amu;
+  double* aT;
   int ntiles, ngroups;
   double* gpart;
   unsigned* gticket;   // [ngroups] arrival counters

@@ -152,6 +152,18 @@ class DeviceGrid:
                                           stream_handle()), "tdgl_observables")
         return dict(zip(("psi2", "Bx", "By", "Bz", "Jx", "Jy", "Jz"), outs))
 
+    def adjoint_solve(self, x: torch.Tensor, b: torch.Tensor, h: float, tol: float, B=(0.0, 0.0, 0.0)):
+        """(I - h J(x)^T) mu = b on the device (FP64 context): (mu, iterations,
+        converged); at kmax iterations without convergence, mu is the last
+        iterate."""
+        mu = self.empty_state()
+        it = C.c_int32(0)
+        rc = self.lib.tdgl_adjoint_solve(self.handle, _ptr(x), _ptr(b), _ptr(mu), float(h), float(tol),
+                                         *map(float, B), C.byref(it), stream_handle())
+        if rc not in (L.TDGL_OK, L.TDGL_ENOCONV):
+            L.check(rc, "tdgl_adjoint_solve")
+        return mu, int(it.value), rc == L.TDGL_OK
+
     def plaquette_winding(self, x: torch.Tensor, mask_threshold: float) -> torch.Tensor:
         """Winding numbers of all plaquettes: (slices, Nx-2, Ny-2), NaN where masked."""
         p = self.params
