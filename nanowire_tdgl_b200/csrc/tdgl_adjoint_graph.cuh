@@ -7,8 +7,12 @@
 // on the raw basis.  Control decisions stay on the device; the host reads the
 // outcome once, after the solve.
 //
-//   init, init_fin, KRYLOV while { zero, vjp, combine, dots, fin_dots, orth,
-//   fin_orth }, solve, update
+//   ONCE while { init, init_fin, KRYLOV while { zero, vjp, combine, dots,
+//   fin_dots, orth, fin_orth }, solve, update, end }
+//
+// (the outer loop runs once; its handle also stands for the Newton handle
+// that the shared kernels clear when they abort, so every handle of the
+// graph drives a conditional node)
 //
 // The solve stops at the GMRES tolerance or at kmax iterations (no restart);
 // the caller restarts on the host from the returned iterate if needed.
@@ -117,6 +121,11 @@ __global__ void kg_adj_solve(GArgs<double> A) {
   for (int i = 0; i < j; ++i) cj[i] = y[i] * sj[i];
 }
 
+// End of the single pass of the outer loop.
+__global__ void kg_adj_end(GArgs<double> A) {
+  if (threadIdx.x == 0) cudaGraphSetConditional(A.h_step, 0);
+}
+
 // mu = sum_i c_i v~_i.
 __global__ void __launch_bounds__(kThreads) kg_adj_update(GArgs<double> A) {
   const GDev* d = A.dev;
@@ -135,18 +144,18 @@ cudaError_t build_adjoint_graph(GArgs<double> A, cudaGraph_t* out_graph, cudaGra
   cudaGraph_t G;
   TDGL_GCK(cudaGraphCreate(&G, 0));
   *out_graph = G;
-  // the step and Newton handles are never set to 1 here; the shared kernels'
-  // abort path clears them
-  TDGL_GCK(cudaGraphConditionalHandleCreate(&A.h_step, G, 0, 0));
-  TDGL_GCK(cudaGraphConditionalHandleCreate(&A.h_newton, G, 0, 0));
+  TDGL_GCK(cudaGraphConditionalHandleCreate(&A.h_step, G, 1, cudaGraphCondAssignDefault));
+  A.h_newton = A.h_step;
   TDGL_GCK(cudaGraphConditionalHandleCreate(&A.h_krylov, G, 0, 0));
   const int nb = A.nblk;
   const size_t fin_smem = (size_t)(A.kmax + 1) * sizeof(double);
   Chain top{G};
-  TDGL_GCK(top.kernel((const void*)kg_adj_init, nb, kThreads, 0, A));
-  TDGL_GCK(top.kernel((const void*)kg_adj_init_fin, 1, kThreads, 0, A));
-  cudaGraph_t body;
-  TDGL_GCK(top.loop(A.h_krylov, &body));
+  cudaGraph_t once, body;
+  TDGL_GCK(top.loop(A.h_step, &once));
+  Chain co{once};
+  TDGL_GCK(co.kernel((const void*)kg_adj_init, nb, kThreads, 0, A));
+  TDGL_GCK(co.kernel((const void*)kg_adj_init_fin, 1, kThreads, 0, A));
+  TDGL_GCK(co.loop(A.h_krylov, &body));
   Chain ck{body};
   TDGL_GCK(ck.kernel((const void*)kg_adj_zero, nb, kThreads, 0, A));
   TDGL_GCK(ck.kernel((const void*)kg_adj_vjp<D3>, nb, kThreads, 0, A));
@@ -155,8 +164,9 @@ cudaError_t build_adjoint_graph(GArgs<double> A, cudaGraph_t* out_graph, cudaGra
   TDGL_GCK(ck.kernel((const void*)kg_fin_dots<double>, 1, kThreads, fin_smem, A));
   TDGL_GCK(ck.kernel((const void*)kg_orth<double, D3>, nb, kThreads, 0, A));
   TDGL_GCK(ck.kernel((const void*)kg_fin_orth<double>, 1, kThreads, 0, A));
-  TDGL_GCK(top.kernel((const void*)kg_adj_solve, 1, kThreads, 0, A));
-  TDGL_GCK(top.kernel((const void*)kg_adj_update, nb, kThreads, 0, A));
+  TDGL_GCK(co.kernel((const void*)kg_adj_solve, 1, kThreads, 0, A));
+  TDGL_GCK(co.kernel((const void*)kg_adj_update, nb, kThreads, 0, A));
+  TDGL_GCK(co.kernel((const void*)kg_adj_end, 1, kThreads, 0, A));
   TDGL_GCK(cudaGraphInstantiate(out_exec, G, 0));
   return cudaSuccess;
 }
