@@ -1050,12 +1050,14 @@ __global__ void __launch_bounds__(kThreads, 4) kg_arn_dots(GArgs<T> A) {
   // one sweep over the entries: Z is read once per entry and every vector is
   // combined with it there; the warp adds its 32 products per vector and
   // lane 0 accumulates the warp's sums in double (all lanes stay in the loop:
-  // its bound is warp-uniform)
+  // its bound is warp-uniform).  The sweep runs from the last entry down: the
+  // orthogonalisation and the product before it swept upwards, so the top
+  // entries of the basis are the ones still in L2 when this kernel starts.
   const long wq0 = blockIdx.x * (long)blockDim.x + (threadIdx.x & ~31);
-  long mo = (4 * (wq0 + lane)) % npf;
+  long mo = (4 * max(nq - 1 - (wq0 + lane), 0L)) % npf;
   for (long qb = wq0; qb < nq; qb += stride) {
-    const long q = qb + lane;
-    const bool ok = q < nq;
+    const long q = nq - 1 - (qb + lane);
+    const bool ok = q >= 0;
     const long e = 4 * q;
     V4<T> z = ok ? ld4(Z + e) : V4<T>{0, 0, 0, 0};
     if (ok) {
@@ -1077,8 +1079,8 @@ __global__ void __launch_bounds__(kThreads, 4) kg_arn_dots(GArgs<T> A) {
         if (lane == 0) red[warp * nd + i0 + t] += (double)p;
       }
     }
-    mo += 4 * stride;
-    while (mo >= npf) mo -= npf;
+    mo -= 4 * stride;
+    while (mo < 0) mo += npf;
   }
   __syncthreads();
   for (int s = threadIdx.x; s <= ja; s += blockDim.x) {
