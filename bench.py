@@ -98,7 +98,7 @@ def measured_peak():
 # algorithmic bytes (per-stage compulsory traffic, stage counts from the device)
 # ---------------------------------------------------------------------------
 
-def algorithmic_bytes(n_int: int, precision: str, st: dict) -> float:
+def algorithmic_bytes(n_int: int, precision: str, st: dict, poly_deg: int = 0) -> float:
     """Compulsory HBM bytes of the counted work.
 
     S64 = 40 B/node (psi complex + 3 real links, FP64 state), SK = bytes/node
@@ -114,22 +114,32 @@ def algorithmic_bytes(n_int: int, precision: str, st: dict) -> float:
     (m^2 + 8 m + 7) SK (orthogonalisation j + 2 vectors, product 3,
     projections j + 2; one more step than iterations), within a few percent of
     the model at m ~ 25, and the measured DRAM traffic is 0.93 x the model.
+    With the polynomial preconditioner of degree d, every Arnoldi column and
+    every Newton correction takes d more stencil launches (counted in
+    jvp_evals, 3 SK + F each) that also read the vector they precondition
+    (+SK each), and the correction is first combined from the basis
+    (m + 1 vectors per Newton iteration).
     """
     S64 = 40.0 * n_int
     SK = (20.0 if precision == "mixed" else 40.0) * n_int
     F = 1.0 * n_int
+    poly = poly_deg * (st["krylov_iters"] + st["newton_iters"]) * SK
+    if poly_deg:
+        poly += (st["krylov_iters"] + st["newton_iters"]) * SK
     return (st["rhs_evals"] * (2 * S64 + F) + st["jvp_evals"] * (3 * SK + F)
-            + (st["krylov_sq"] + 7 * st["krylov_iters"]) * SK + 7 * S64 * st["newton_iters"])
+            + (st["krylov_sq"] + 7 * st["krylov_iters"]) * SK + 7 * S64 * st["newton_iters"] + poly)
 
 
-def graph_launches(st: dict, jvp: str) -> int:
+def graph_launches(st: dict, jvp: str, poly_deg: int = 0) -> int:
     """Kernel launches of the step graph: 7 per step attempt, 4 per Newton
     iteration, and per Krylov solve of m iterations either 3 (m + 1)
     (orthogonalisation, product, projections; analytic products) or 5 m
-    (finite-difference products)."""
+    (finite-difference products); with the polynomial preconditioner of
+    degree d, d more per Arnoldi step and d + 1 more per Newton iteration."""
     base = 7 * (st["steps"] + st["rejections"]) + 4 * st["newton_iters"]
     if jvp == "analytic":
-        return base + 3 * (st["krylov_iters"] + st["newton_iters"])
+        return (base + (3 + poly_deg) * (st["krylov_iters"] + st["newton_iters"])
+                + (poly_deg + 1 if poly_deg else 0) * st["newton_iters"])
     return base + 5 * st["krylov_iters"]
 
 
@@ -275,7 +285,8 @@ def run_ours(a, rank, world):
     value = job_rate(a.steps, world, ms_max)
 
     peak, peak_kind = measured_peak()
-    alg = algorithmic_bytes(n_int, a.precision, st)
+    poly_deg = g.poly_degree if (jvp == "analytic" and a.krylov == "gmres") else 0
+    alg = algorithmic_bytes(n_int, a.precision, st, poly_deg)
     achieved = alg / (ms / 1e3) / 1e9
     # DRAM bytes per algorithmic byte of the GMRES step graph, measured with ncu
     # (graph-level dram__bytes_read.sum + dram__bytes_write.sum) on a 2-step
@@ -288,11 +299,12 @@ def run_ours(a, rank, world):
         "vs_baseline": None, "dtype": "f32 Krylov / f64 state" if a.precision == "mixed" else "f64",
         "data": "synthetic (seeded psi0 noise, phi0 = 0; no dataset involved)",
         "config": {"workload": WORKLOAD_NAME, "precision": a.precision, "jvp": jvp, "krylov": a.krylov,
+                   "preconditioner": f"Chebyshev polynomial, degree {poly_deg}" if poly_deg else "none",
                    "n_interior": n_int,
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": "inputs larger than L2: Krylov basis of ~2x26 state vectors (>0.5 GB) per solve"},
         "node_updates_per_s": value * n_int,
-        "gpu_launches": graph_launches(st, jvp) if a.krylov == "gmres" else 1,
+        "gpu_launches": graph_launches(st, jvp, poly_deg) if a.krylov == "gmres" else 1,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_kind": peak_kind,
                      "algorithmic_bytes_per_launch": alg,
@@ -692,7 +704,7 @@ def run_trilayer(a):
     def rel(k):
         return float(torch.linalg.vector_norm(om[k] - od[k]) / torch.linalg.vector_norm(od[k]))
     peak, peak_kind = measured_peak()
-    alg = algorithmic_bytes(n_int, "mixed", stm)
+    alg = algorithmic_bytes(n_int, "mixed", stm, gm.poly_degree)
     achieved = alg / (msm / 1e3) / 1e9
     return {"form": "trilayer", "metric": "trapezoidal steps/s, 256x256x64 S/I/S trilayer, mixed vs FP64",
             "value": a.steps / (msm / 1e3), "unit": "steps/s", "steps": a.steps, "warmup": a.warmup,

@@ -225,7 +225,8 @@ int tdgl_adjoint_solve(tdgl_ctx* ctx, const double* x_dev, const double* b_dev, 
  * tdgl_trap_collect returns the clock, step size, counters and status.  One
  * uncollected launch per context at a time; while it is pending, the
  * context's other stepping entry points (tdgl_trap_run, tdgl_newton_trap,
- * tdgl_tgcr_trap, tdgl_euler_run, tdgl_arnoldi_probe, tdgl_ctx_set_blocks)
+ * tdgl_tgcr_trap, tdgl_euler_run, tdgl_arnoldi_probe, tdgl_ctx_set_blocks,
+ * tdgl_ctx_set_poly)
  * return TDGL_EINVAL, as they share its workspace. */
 int tdgl_trap_launch(tdgl_ctx* ctx, double* x_dev, double t, double dt_cur, int32_t max_steps,
                      const tdgl_trap_opts* opts, const tdgl_field* field, tdgl_stream_t stream);
@@ -239,6 +240,19 @@ int tdgl_trap_collect(tdgl_ctx* ctx, double* t, double* dt_cur, tdgl_stats* stat
  * (small instances run concurrently on few blocks each); the graph is rebuilt
  * at the next launch.  No reference counterpart. */
 int tdgl_ctx_set_blocks(tdgl_ctx* ctx, int32_t stream_blocks, int32_t krylov_blocks, int32_t fused);
+/* Degree (0 to 8) of the polynomial right preconditioner of the GMRES solves
+ * with analytic Jacobian products: GMRES runs on A p(A), A = I - dt/2 J,
+ * p the Chebyshev-iteration polynomial of that degree for the interval
+ * [1 - dt/2, 1 + dt/2 rho], rho a Gershgorin bound of J; the Newton
+ * correction is p(A) times the Krylov combination, so the stop test and the
+ * solution are those of the unpreconditioned system.  0 turns it off, -1
+ * restores the default (3, or TDGL_POLY_DEGREE).  The finite-difference
+ * (reference) form never uses it.  The graph is rebuilt at the next launch;
+ * TDGL_EINVAL while a launch is pending.  No reference counterpart (the
+ * reference's GCR is unpreconditioned). */
+int tdgl_ctx_set_poly(tdgl_ctx* ctx, int32_t degree);
+/* Degree in use (or that the next graph will use); -1 for a null context. */
+int32_t tdgl_ctx_poly_degree(const tdgl_ctx* ctx);
 /* Forward Euler: n_steps steps of min(dt, t_stop - t) from *t (updated)
  * (src/tdgl3d/solvers/integrators.py:35-89). */
 int tdgl_euler_run(tdgl_ctx* ctx, double* x_dev, double* t, double t_stop, double dt, int32_t n_steps,

@@ -87,6 +87,8 @@ SIGNATURES = {
     "tdgl_trap_launch": (C.c_int, [_P, _P, _D, _D, _I, C.POINTER(TrapOpts), C.POINTER(Field), _P]),
     "tdgl_trap_collect": (C.c_int, [_P, C.POINTER(_D), C.POINTER(_D), C.POINTER(Stats)]),
     "tdgl_ctx_set_blocks": (C.c_int, [_P, _I, _I, _I]),
+    "tdgl_ctx_set_poly": (C.c_int, [_P, _I]),
+    "tdgl_ctx_poly_degree": (C.c_int32, [_P]),
     "tdgl_euler_run": (C.c_int, [_P, _P, C.POINTER(_D), _D, _D, _I, C.POINTER(Field), _P]),
     "tdgl_vjp": (C.c_int, [_P, _P, _P, _D, _D, _D, _P, _P, _P, _P, _P]),
     "tdgl_profile": (C.c_int, [_P, C.POINTER(C.c_uint64), C.c_int64, _I]),

@@ -35,6 +35,8 @@ cudaError_t arnoldi_probe_f64(const GArgs<double>& A, int launches, int kernels,
 static constexpr long kProfLen = 64 + 2 * 1024;
 // upper bound of the step graph's blocks per SM (its partial-sum buffers are sized for it)
 static constexpr int kMaxBlocksPerSm = 8;
+// default degree of the polynomial preconditioner (analytic-product GMRES)
+static constexpr int kPolyDefault = 3;
 
 namespace {
 
@@ -128,6 +130,13 @@ struct tdgl_ctx {
   int apply_dots_req = -1;       // set by tdgl_ctx_set_blocks (-1: the default)
   int nblk_arn = 0, nblk_orth = 0, arn_gx = 0, arn_gy = 0;
   int blk_stream = 0, blk_krylov = 0;   // blocks of the graph's grid kernels (0: defaults)
+  // polynomial preconditioner of the analytic-product solves: requested degree
+  // (-1: the default), the degree in use, the largest kappa^2 of the grid, and
+  // the Horner buffers / Newton correction (full-grid vectors)
+  int poly_req = -1, poly_deg = 0;
+  double k2max = 0.0;
+  void* PW[2] = {nullptr, nullptr};
+  void* PC = nullptr;
   bool pending = false, pending_noop = false;   // an uncollected tdgl_trap_launch
   uint8_t* imask = nullptr;
   uint32_t* deadmask = nullptr;   // per interior node: dead links read by the Arnoldi product
@@ -220,6 +229,8 @@ extern "C" int tdgl_ctx_create(const tdgl_grid_desc* gd, const tdgl_material_des
     TDGL_CUDA(cudaMemcpy(c->k2, hg.k2.data(), n * sizeof(double), cudaMemcpyHostToDevice));
   }
   g.k2int = c->k2;
+  c->k2max = g.kappa2;
+  if (!hg.k2.empty()) c->k2max = *std::max_element(hg.k2.begin(), hg.k2.end());
   if (!hg.sc.empty()) {
     if ((rc = ctx_alloc(c, (void**)&c->sc, n * sizeof(double)))) { tdgl_ctx_destroy(c); return rc; }
     TDGL_CUDA(cudaMemcpy(c->sc, hg.sc.data(), n * sizeof(double), cudaMemcpyHostToDevice));
@@ -626,6 +637,29 @@ extern "C" int tdgl_newton_trap(tdgl_ctx* c, double* x, const double* gamma, dou
 // Graph executor (GMRES): workspace, graph, launch
 // ---------------------------------------------------------------------------
 
+// Degree of the polynomial preconditioner: tdgl_ctx_set_poly, else
+// TDGL_POLY_DEGREE, else the default.
+static int poly_setting(const tdgl_ctx* c) {
+  int d = kPolyDefault;
+  if (c->poly_req >= 0) d = c->poly_req;
+  else if (const char* e = std::getenv("TDGL_POLY_DEGREE")) {
+    if (e[0]) d = std::atoi(e);
+  }
+  return std::min(std::max(d, 0), kPolyMax);
+}
+
+// Upper bound of the spectral radius of J (Gershgorin, from the stencil
+// coefficients): the vector-potential rows sum to at most 8 kappa^2 sum_a 1/h_a^2
+// plus the supercurrent terms (|psi|^2 of order 1), the order-parameter rows
+// to (2 + 2 sqrt 2) sum_a 1/h_a^2 plus the nonlinear and relaxation terms.
+static double poly_rho_bound(const tdgl_ctx* c) {
+  const Grid& g = c->g;
+  const double s2 = 1.0 / g.hx2 + 1.0 / g.hy2 + (g.is3d ? 1.0 / g.hz2 : 0.0);
+  const double field = 8.0 * c->k2max * s2 + 6.0;
+  const double order = (2.0 + 2.0 * std::sqrt(2.0)) * s2 + 4.0 + (g.has_material ? 1.0 / kTauRelax : 0.0);
+  return 1.02 * std::max(field, order);
+}
+
 template <typename T>
 static GArgs<T> make_gargs(tdgl_ctx* c) {
   GArgs<T> A{};
@@ -670,6 +704,11 @@ static GArgs<T> make_gargs(tdgl_ctx* c) {
   A.cxu = c->g.kappa2 / c->g.hx2;
   A.cyu = c->g.kappa2 / c->g.hy2;
   A.czu = c->g.is3d ? c->g.kappa2 / c->g.hz2 : 0.0;
+  A.poly_deg = c->UB ? c->poly_deg : 0;
+  A.poly_rho = poly_rho_bound(c);
+  A.PW[0] = (T*)c->PW[0];
+  A.PW[1] = (T*)c->PW[1];
+  A.PC = (T*)c->PC;
   return A;
 }
 
@@ -721,6 +760,10 @@ static int ensure_arnoldi_ws(tdgl_ctx* c) {
   if ((rc = ctx_alloc(c, &c->UB, vb * (c->kmax + 1)))) return rc;
   if ((rc = ctx_alloc(c, &c->Zb[0], vb))) return rc;
   if ((rc = ctx_alloc(c, &c->Zb[1], vb))) return rc;
+  if ((rc = ctx_alloc(c, &c->PW[0], vb))) return rc;
+  if ((rc = ctx_alloc(c, &c->PW[1], vb))) return rc;
+  if ((rc = ctx_alloc(c, &c->PC, vb))) return rc;
+  c->poly_deg = poly_setting(c);
   const size_t nparts = std::max((size_t)c->num_sms * kMaxBlocksPerSm, (size_t)c->ntiles);
   if ((rc = ctx_alloc(c, (void**)&c->part_arn, sizeof(double) * (c->kmax + 2) * nparts))) return rc;
   if ((rc = ctx_alloc(c, (void**)&c->gpart, sizeof(double) * (c->kmax + 2) * (size_t)c->ngroups_cap))) return rc;
@@ -797,10 +840,12 @@ static int ensure_graph(tdgl_ctx* c, int v) {
   if (c->precision == TDGL_MIXED) {
     GArgs<float> A = make_gargs<float>(c);
     A.fused = v;
+    if (!v) A.poly_deg = 0;
     e = graph_build_f32(A, &c->graph[v], &c->gexec[v]);
   } else {
     GArgs<double> A = make_gargs<double>(c);
     A.fused = v;
+    if (!v) A.poly_deg = 0;
     e = graph_build_f64(A, &c->graph[v], &c->gexec[v]);
   }
   if (e != cudaSuccess) {
@@ -998,6 +1043,24 @@ extern "C" int tdgl_ctx_set_blocks(tdgl_ctx* c, int32_t stream_blocks, int32_t k
     c->graph[v] = nullptr;
   }
   return TDGL_OK;
+}
+
+extern "C" int tdgl_ctx_set_poly(tdgl_ctx* c, int32_t degree) {
+  if (!c) return fail(TDGL_EINVAL, "null argument");
+  if (degree < -1 || degree > kPolyMax) return fail(TDGL_EINVAL, "polynomial degree must lie in [-1, 8]");
+  if (c->pending) return fail(TDGL_EINVAL, "a launch of this context has not been collected");
+  c->poly_req = degree;
+  if (c->UB) c->poly_deg = poly_setting(c);
+  if (c->gexec[1]) cudaGraphExecDestroy(c->gexec[1]);   // the analytic-product graph is rebuilt at the next launch
+  if (c->graph[1]) cudaGraphDestroy(c->graph[1]);
+  c->gexec[1] = nullptr;
+  c->graph[1] = nullptr;
+  return TDGL_OK;
+}
+
+extern "C" int32_t tdgl_ctx_poly_degree(const tdgl_ctx* c) {
+  if (!c) return -1;
+  return c->UB ? c->poly_deg : poly_setting(c);
 }
 
 extern "C" int tdgl_trap_run(tdgl_ctx* c, double* x, double* t, double* dt_cur, int32_t max_steps,

@@ -40,6 +40,8 @@ enum GStatus : int { GS_OK = 0, GS_NOCONV = 1, GS_DTMIN = 2, GS_KMAX = 3, GS_NON
 constexpr int kKTypes = 16;   // slots of the per-kernel timers
 
 // Device control block of the graph executor.
+constexpr int kPolyMax = 8;   // highest degree of the polynomial preconditioner
+
 struct GDev {
   // inputs for one launch
   double t, dt_cur, t_stop, dt, dt_min, tol_f, tol_dx, tol_gcr, eps_mf;
@@ -54,6 +56,10 @@ struct GDev {
   long long newton_iters, krylov_iters, krylov_sq, rhs_evals, jvp_evals, rejections;
   int max_krylov, krylov_last;
   int ja;                          // basis vector the next Arnoldi step forms
+  // polynomial preconditioner of the analytic-product Krylov solves (set per
+  // step from dta): p(lambda) = sum_k poly_e[k] t^k, t = (lambda - theta) / delta
+  double poly_e[kPolyMax + 1];
+  double poly_theta, poly_delta;
   // per-kernel timers (diagnostics, on when prof_on): first block start to
   // last block end of each launch, summed per kernel type
   int prof_on;
@@ -133,6 +139,16 @@ struct GArgs {
   int ntiles, ngroups;
   double* gpart;
   unsigned* gticket;   // [ngroups] arrival counters
+  // polynomial right preconditioner of the analytic-product solves: degree
+  // (0: none), an upper bound of the spectral radius of J, the Horner buffers
+  // (ping-pong) and the Newton correction before the polynomial; pstep / pmode
+  // are per kernel node (Horner step; 0: Krylov direction U_ja, 1: correction)
+  int poly_deg;
+  double poly_rho;
+  T* PW[2];
+  T* PC;
+  int pstep, pmode;
+  int upd_single;      // kg_update_fused adds PW[0] (the preconditioned correction) alone
 };
 
 template <typename T> __host__ __device__ __forceinline__ double* kry_sj(const GArgs<T>& A) { return A.kry; }
@@ -657,8 +673,12 @@ __global__ void __launch_bounds__(kThreads, 3) kg_update_fused(GArgs<T> A) {
   kt_begin(A.dev, KT_UPDATE);
   constexpr int NC = D3 ? 5 : 4;
   const Grid& g = A.g;
-  const int nk = d->j;
-  const double* cj = kry_cj(A);
+  // with the polynomial preconditioner the correction p(A) sum_i c_i U_i is
+  // already formed in PW[0]: one vector with coefficient 1
+  const double one[4] = {1.0, 0.0, 0.0, 0.0};
+  const int nk = A.upd_single ? 1 : d->j;
+  const double* cj = A.upd_single ? one : kry_cj(A);
+  const T* UBase = A.upd_single ? A.PW[0] : A.UB;
   const double czxy = d->czxy, cyzx = d->cyzx, cxyz = d->cxyz;
   double acc[1] = {0.0};
   // basis on the full grid: one node per thread
@@ -671,7 +691,7 @@ __global__ void __launch_bounds__(kThreads, 3) kg_update_fused(GArgs<T> A) {
     for (int c = 0; c < NC; ++c) s[c] = 0.0;
     int i0 = 0;
     for (; i0 + 4 <= nk; i0 += 4) {
-      const T* U = A.UB + (long)i0 * A.vs + m;
+      const T* U = UBase + (long)i0 * A.vs + m;
       const double c0 = cj[i0], c1 = cj[i0 + 1], c2 = cj[i0 + 2], c3 = cj[i0 + 3];
 #pragma unroll
       for (int c = 0; c < NC; ++c) {
@@ -681,7 +701,7 @@ __global__ void __launch_bounds__(kThreads, 3) kg_update_fused(GArgs<T> A) {
       }
     }
     for (; i0 < nk; ++i0) {
-      const T* U = A.UB + (long)i0 * A.vs + m;
+      const T* U = UBase + (long)i0 * A.vs + m;
 #pragma unroll
       for (int c = 0; c < NC; ++c) s[c] += cj[i0] * (double)U[(long)c * A.npf];
     }
@@ -761,7 +781,7 @@ __device__ void arn_finish(const GArgs<T>& A, GDev* d, int ja, const double* S) 
     const double un = sqrt(S[ja + 1]);
     const double hn = un;                                // h_{jc, jc-1} = ||A v - sum h v|| = ||U_jc||
     sj[jc] = un > 0.0 ? 1.0 / un : 0.0;
-    d->jvp_evals += 1;
+    d->jvp_evals += 1 + A.poly_deg;
     col[jc] = hn;
     for (int i = 0; i + 1 < jc; ++i) {
       double a = col[i], b = col[i + 1];
@@ -930,7 +950,8 @@ __global__ void __launch_bounds__(kThreads, 3) kg_arn_apply(GArgs<T> A) {
   const Grid& g = A.g;
   const int ja = d->ja;
   const long npf = A.npf;
-  const T* Uj = A.UB + (long)ja * A.vs;
+  // product input: U_ja, or p(A) U_ja from the polynomial steps
+  const T* Uj = A.poly_deg > 0 ? A.PW[0] : A.UB + (long)ja * A.vs;
   T* Zout = A.Zb[ja & 1];
   const double dth = d->dta / 2.0;
   const int i = 1 + blockIdx.x * 32 + (threadIdx.x & 31), j = 1 + blockIdx.y * 8 + (threadIdx.x >> 5);
@@ -958,6 +979,130 @@ __global__ void __launch_bounds__(kThreads, 3) kg_arn_apply(GArgs<T> A) {
     write_eff<T, D3, true>(g, Zout, npf, i, j, k, z, 0.0, 0.0, 0.0);
   }
   kt_end(d, KT_ARN_APPLY);
+}
+
+// Polynomial right preconditioner of the analytic-product solves.  The
+// trapezoidal operator A = I - dt/2 J(x) has its spectrum in [a, b] with
+// a = 1 - dt/2 (J's eigenvalues are at most 1: the (1 - |psi|^2) psi term)
+// and b = 1 + dt/2 rho, rho a Gershgorin bound of J from the stencil
+// coefficients.  p is the Chebyshev-iteration polynomial of degree d for that
+// interval, p(lambda) = (1 - T_{d+1}((theta - lambda) / delta) / T_{d+1}(theta / delta)) / lambda,
+// theta = (a + b) / 2, delta = (b - a) / 2, so that lambda p(lambda) lies within
+// 1 +- 1 / T_{d+1}(theta / delta) on [a, b]; GMRES then runs on A p(A), and the
+// Newton correction is p(A) applied to the Krylov combination.  p is stored in
+// the centred variable t = (lambda - theta) / delta (|t| <= 1 on [a, b]) and
+// applied by Horner's rule, one stencil launch per degree.
+template <typename T>
+__device__ void poly_setup(const GArgs<T>& A, GDev* d) {
+  const int n = A.poly_deg + 1;
+  const double h = d->dta / 2.0;
+  double* e = d->poly_e;
+  for (int k = 0; k <= kPolyMax; ++k) e[k] = 0.0;
+  const double a = 1.0 - h, b = 1.0 + h * A.poly_rho;
+  if (!(a > 0.05) || !(b > a)) {                 // no usable interval: p = 1
+    e[0] = 1.0;
+    d->poly_theta = 1.0;
+    d->poly_delta = 1.0;
+    return;
+  }
+  const double th = 0.5 * (a + b), de = 0.5 * (b - a), x0 = th / de;
+  // T_n(-t) in powers of t by the three-term recurrence, and T_n(x0)
+  double tm[kPolyMax + 2] = {1.0}, tc[kPolyMax + 2] = {0.0, -1.0}, tn[kPolyMax + 2];
+  double vm = 1.0, vc = x0;
+  for (int m = 1; m < n; ++m) {
+    for (int k = 0; k <= m + 1; ++k) tn[k] = (k > 0 ? -2.0 * tc[k - 1] : 0.0) - (k <= m - 1 ? tm[k] : 0.0);
+    for (int k = 0; k <= m + 1; ++k) { tm[k] = tc[k]; tc[k] = tn[k]; }
+    const double vn = 2.0 * x0 * vc - vm;
+    vm = vc;
+    vc = vn;
+  }
+  // N(t) = 1 - T_n(-t) / T_n(x0) vanishes at t0 = -x0 (lambda = 0); p = N / (delta (t - t0))
+  double N[kPolyMax + 2];
+  for (int k = 0; k <= n; ++k) N[k] = -tc[k] / vc;
+  N[0] += 1.0;
+  const double t0 = -x0;
+  double q = N[n];
+  e[n - 1] = q / de;
+  for (int k = n - 1; k >= 1; --k) {
+    q = N[k] + t0 * q;
+    e[k - 1] = q / de;
+  }
+  d->poly_theta = th;
+  d->poly_delta = de;
+}
+
+// One Horner step of the preconditioner on the full grid:
+//   W_k = e_k V + beta t(W_in),  t(W) = (A W - theta W) / delta,
+// V = U_ja (Krylov direction, pmode 0) or the Newton correction PC (pmode 1);
+// the first step (k = d - 1) starts from W_in = V with beta = e_d, the others
+// read W_{k+1} with beta = 1.  The stencil is the product kernel's (dead
+// links from the per-node mask); W_k is written with its face values.
+template <typename T, bool D3>
+__global__ void __launch_bounds__(kThreads, 3) kg_arn_poly(GArgs<T> A) {
+  GDev* d = A.dev;
+  if (!gdev_ok(d)) return;
+  if (A.pmode && d->newton_failed) return;
+  kt_begin(d, KT_ARN_APPLY);
+  constexpr int NC = D3 ? 5 : 4;
+  const Grid& g = A.g;
+  const long npf = A.npf;
+  const int kst = A.pstep, deg = A.poly_deg;
+  const T* V = A.pmode ? A.PC : A.UB + (long)d->ja * A.vs;
+  const T* Win = kst == deg - 1 ? V : A.PW[(kst + 1) & 1];
+  T* Wout = A.PW[kst & 1];
+  const double alpha = d->poly_e[kst], beta = kst == deg - 1 ? d->poly_e[deg] : 1.0;
+  const double th = d->poly_theta, ide = 1.0 / d->poly_delta, dth = d->dta / 2.0;
+  const int i = 1 + blockIdx.x * 32 + (threadIdx.x & 31), j = 1 + blockIdx.y * 8 + (threadIdx.x >> 5);
+  const int k = D3 ? 1 + (int)blockIdx.z : 0;
+  if (i <= g.nx && j <= g.ny) {
+    const int n = dix(g, i, j, k);
+    const long m = full_index(g, i, j, k);
+    const uint8_t nf = g.nflags[n];
+    NodeCoef<T> nc;
+    if (g.kappa_per_node) nc = node_coef<T>(g, n, nf);
+    else {
+      nc.cx = (T)A.cxu; nc.cy = (T)A.cyu; nc.cz = (T)A.czu;
+      nc.material = g.has_material != 0;
+      if (!nc.material) nc.sc = T(1);
+      else if (nf & NF_SCFRAC) nc.sc = (T)g.scint[n];
+      else nc.sc = (nf & NF_SC0) ? T(0) : T(1);
+    }
+    NbEro<T> X{A.XLe, npf, m, g.mj, g.mk};
+    NbMk<T> P{Win, npf, m, g.mj, g.mk, A.deadmask[n], NbM<T>{Win, npf, m, g.mj, g.mk, i, j, k, &g, g.lflags}};
+    T o[5];
+    jvp_body<T, D3>(g, X, P, nc, nf, o);
+    double z[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      const double w = (double)Win[c * npf + m];
+      z[c] = alpha * (double)V[c * npf + m] + beta * ((w - dth * (double)o[c]) - th * w) * ide;
+    }
+    write_eff<T, D3, true>(g, Wout, npf, i, j, k, z, 0.0, 0.0, 0.0);
+  }
+  kt_end(d, KT_ARN_APPLY);
+}
+
+// Newton correction before the preconditioner: PC = sum_i c_i U_i over every
+// entry of the full-grid vectors (the combination of face values is the face
+// value of the combination); the polynomial steps then form p(A) PC.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) kg_poly_combine(GArgs<T> A) {
+  GDev* d = A.dev;
+  if (!gdev_ok(d) || d->newton_failed) return;
+  if (blockIdx.x == 0 && threadIdx.x == 0) d->jvp_evals += A.poly_deg;
+  const int nk = d->j;
+  const double* cj = kry_cj(A);
+  const long vs = A.vs, nq = vs / 4;
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < nq; q += (long)gridDim.x * blockDim.x) {
+    const long e = 4 * q;
+    double v[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int i = 0; i < nk; ++i) {
+      const V4<T> a = ld4(A.UB + (long)i * vs + e);
+      const double c = cj[i];
+      v[0] += c * (double)a.a; v[1] += c * (double)a.b; v[2] += c * (double)a.c; v[3] += c * (double)a.d;
+    }
+    st4(A.PC + e, v);
+  }
 }
 
 // Blocks of a two-level fold: groups of kTileGroup consecutive blocks.
@@ -1140,7 +1285,8 @@ __global__ void __launch_bounds__(kThreads, 3) kg_arn_apply_dots(GArgs<T> A) {
   const Grid& g = A.g;
   const int ja = d->ja;
   const long npf = A.npf;
-  const T* Uj = A.UB + (long)ja * A.vs;
+  // product input: U_ja, or p(A) U_ja from the polynomial steps
+  const T* Uj = A.poly_deg > 0 ? A.PW[0] : A.UB + (long)ja * A.vs;
   T* Zout = A.Zb[ja & 1];
   const double dth = d->dta / 2.0;
   const int i = 1 + blockIdx.x * 32 + (threadIdx.x & 31), j = 1 + blockIdx.y * 8 + (threadIdx.x >> 5);
@@ -1279,6 +1425,7 @@ __global__ void kg_newton_init(GArgs<T> A) {
   d->rho0 = sqrt(s[0]);
   d->xnorm = sqrt(s[1]);
   if (!isfinite(d->rho0) || !isfinite(d->xnorm)) { abort_all(A, GS_NONFINITE); return; }
+  if (A.poly_deg > 0) poly_setup(A, d);
   bool run_newton = d->newton_max_iter >= 1;
   bool kc = run_newton && krylov_start(A, d);
   cudaGraphSetConditional(A.h_newton, run_newton ? 1 : 0);

@@ -75,8 +75,24 @@ cudaError_t build_trap_graph(GArgs<T> A, cudaGraph_t* out_graph, cudaGraphExec_t
   Chain cn{newton_body};
   TDGL_GCK(cn.loop(A.h_krylov, &krylov_body));
   TDGL_GCK(cn.kernel((const void*)kg_newton_solve<T>, 1, kThreads, 0, A));
-  if (A.fused) TDGL_GCK(cn.kernel((const void*)kg_update_fused<T, D3>, nb, kThreads, 0, A));
-  else TDGL_GCK(cn.kernel((const void*)kg_update<T, D3>, nb, kThreads, 0, A));
+  const dim3 tiles(A.arn_gx, A.arn_gy, D3 ? A.g.nz : 1);
+  if (A.fused && A.poly_deg > 0) {
+    // Newton correction p(A) sum_i c_i U_i, then the update with that one vector
+    TDGL_GCK(cn.kernel((const void*)kg_poly_combine<T>, nb, kThreads, 0, A));
+    for (int k = A.poly_deg - 1; k >= 0; --k) {
+      GArgs<T> P = A;
+      P.pstep = k;
+      P.pmode = 1;
+      TDGL_GCK(cn.kernel((const void*)kg_arn_poly<T, D3>, tiles, kThreads, 0, P));
+    }
+    GArgs<T> U = A;
+    U.upd_single = 1;
+    TDGL_GCK(cn.kernel((const void*)kg_update_fused<T, D3>, nb, kThreads, 0, U));
+  } else if (A.fused) {
+    TDGL_GCK(cn.kernel((const void*)kg_update_fused<T, D3>, nb, kThreads, 0, A));
+  } else {
+    TDGL_GCK(cn.kernel((const void*)kg_update<T, D3>, nb, kThreads, 0, A));
+  }
   TDGL_GCK(cn.kernel((const void*)kg_newton_rhs<T, D3>, nb, kThreads, 0, A));
   TDGL_GCK(cn.kernel((const void*)kg_newton_check<T>, 1, kThreads, 0, A));
   Chain ck{krylov_body};
@@ -86,7 +102,12 @@ cudaError_t build_trap_graph(GArgs<T> A, cudaGraph_t* out_graph, cudaGraphExec_t
     TDGL_GCK(cudaFuncSetAttribute((const void*)kg_arn_orth<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smo));
     TDGL_GCK(cudaFuncSetAttribute((const void*)kg_arn_dots<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smd));
     TDGL_GCK(ck.kernel((const void*)kg_arn_orth<T>, A.nblk_orth, kThreads, smo, A));
-    const dim3 tiles(A.arn_gx, A.arn_gy, D3 ? A.g.nz : 1);
+    for (int k = A.poly_deg - 1; k >= 0; --k) {   // p(A) U_ja into PW[0]
+      GArgs<T> P = A;
+      P.pstep = k;
+      P.pmode = 0;
+      TDGL_GCK(ck.kernel((const void*)kg_arn_poly<T, D3>, tiles, kThreads, 0, P));
+    }
     if (A.apply_dots) {
       const size_t smp = apply_dots_smem<T>(A.kmax);
       TDGL_GCK(cudaFuncSetAttribute((const void*)kg_arn_apply_dots<T, D3>,

@@ -253,6 +253,15 @@ class DeviceGrid:
         L.check(self.lib.tdgl_ctx_set_blocks(self.handle, int(stream_blocks), int(krylov_blocks), int(fused)),
                 "tdgl_ctx_set_blocks")
 
+    def set_poly(self, degree: int) -> None:
+        """Degree of the polynomial preconditioner of the analytic-product GMRES
+        solves (0 off, -1 the default)."""
+        L.check(self.lib.tdgl_ctx_set_poly(self.handle, int(degree)), "tdgl_ctx_set_poly")
+
+    @property
+    def poly_degree(self) -> int:
+        return int(self.lib.tdgl_ctx_poly_degree(self.handle))
+
     def euler_run(self, x: torch.Tensor, t: float, t_stop: float, dt: float, n_steps: int, field: L.Field) -> float:
         tt = C.c_double(t)
         L.check(self.lib.tdgl_euler_run(self.handle, _ptr(x), C.byref(tt), float(t_stop), float(dt), int(n_steps),
