@@ -416,8 +416,8 @@ def arnoldi_probe(a):
     """Standalone launches of the Arnoldi-step kernels at basis index
     a.arnoldi_probe on the workload's context, after two steps that fill the
     basis: the graph's kernels together, then each kernel alone
-    (orthogonalisation, product, projections, fused product and projections);
-    prints their times."""
+    (orthogonalisation, product, projections, fused product and projections,
+    the polynomial preconditioner's steps); prints their times."""
     import torch
     from nanowire_tdgl_b200 import _lib as L
     from nanowire_tdgl_b200.engine import grid_for, stream_handle
@@ -434,8 +434,11 @@ def arnoldi_probe(a):
     j = a.arnoldi_probe
     reps = max(a.steps, 1)
     res = {}
+    deg = g.poly_degree
     for name, mask in (("graph", 0), ("orthogonalisation", 1), ("product", 2), ("projections", 4),
-                       ("product_and_projections", 8)):
+                       ("product_and_projections", 8), ("polynomial_steps", 16)):
+        if mask == 16 and deg == 0:
+            continue
         L.check(g.lib.tdgl_arnoldi_probe(g.handle, j, 2, mask, stream_handle()), "tdgl_arnoldi_probe")
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
@@ -445,11 +448,13 @@ def arnoldi_probe(a):
         torch.cuda.synchronize()
         res[name] = e0.elapsed_time(e1) * 1e3 / reps
     vec = dev.params.n_interior * (20 if a.precision == "mixed" else 40)
-    alg = (2 * j + 7) * vec
-    print(json.dumps({"arnoldi_probe": j, "precision": a.precision, "us_per_launch": res,
+    alg = (2 * j + 7 + 4 * deg) * vec
+    print(json.dumps({"arnoldi_probe": j, "precision": a.precision, "poly_degree": deg, "us_per_launch": res,
                       "algorithmic_bytes": alg, "achieved_gbs_graph": alg / (res["graph"] * 1e-6) / 1e9,
-                      "note": "graph kernels together: orthogonalisation (j+2 vectors), product (3), projections "
-                              "(j+2); vector = n_interior x 20 B (FP32)"}))
+                      "note": "graph kernels together: orthogonalisation (j+2 vectors), polynomial steps (4 each: "
+                              "input, direction, output, state), product (3), projections (j+2); "
+                              "polynomial_steps = all deg steps of one Arnoldi step; vector = n_interior x 20 B "
+                              "(FP32)"}))
     return 0
 
 

@@ -293,7 +293,8 @@ int tdgl_profile(tdgl_ctx* ctx, uint64_t* out, int64_t n, int32_t reset);
  * products) outside the graph, forming basis vector ja from whatever the
  * workspace holds, without the Krylov bookkeeping; synchronises the stream.
  * kernels selects what runs (bit 0 orthogonalisation, bit 1 product, bit 2
- * projections, bit 3 fused product and projections; 0 = the graph's own).
+ * projections, bit 3 fused product and projections, bit 4 the polynomial
+ * preconditioner's steps; 0 = the graph's own).
  * For timing and profiling the kernels alone.  No reference counterpart. */
 int tdgl_arnoldi_probe(tdgl_ctx* ctx, int32_t ja, int32_t launches, int32_t kernels, tdgl_stream_t stream);
 
