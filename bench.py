@@ -136,13 +136,14 @@ def algorithmic_bytes(n_int: int, precision: str, st: dict, poly_deg: int = 0) -
 
 def graph_launches(st: dict, jvp: str, poly_deg: int = 0) -> int:
     """Kernel launches of the step graph: 7 per step attempt, 4 per Newton
-    iteration, and per Krylov solve of m iterations either 3 (m + 1)
-    (orthogonalisation, product, projections; analytic products) or 5 m
+    iteration, and per Krylov solve of m iterations either 4 (m + 1)
+    (orthogonalisation, stop check, product, projections; analytic products;
+    the last step's product and projections return at once) or 5 m
     (finite-difference products); with the polynomial preconditioner of
     degree d, d more per Arnoldi step and d + 1 more per Newton iteration."""
     base = 7 * (st["steps"] + st["rejections"]) + 4 * st["newton_iters"]
     if jvp == "analytic":
-        return (base + (3 + poly_deg) * (st["krylov_iters"] + st["newton_iters"])
+        return (base + (4 + poly_deg) * (st["krylov_iters"] + st["newton_iters"])
                 + (poly_deg + 1 if poly_deg else 0) * st["newton_iters"])
     return base + 5 * st["krylov_iters"]
 

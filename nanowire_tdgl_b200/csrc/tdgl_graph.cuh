@@ -56,6 +56,7 @@ struct GDev {
   long long newton_iters, krylov_iters, krylov_sq, rhs_evals, jvp_evals, rejections;
   int max_krylov, krylov_last;
   int ja;                          // basis vector the next Arnoldi step forms
+  int arn_stop;                    // the solve stopped at this Arnoldi step's check: its products are skipped
   // polynomial preconditioner of the analytic-product Krylov solves (set per
   // step from dta): p(lambda) = sum_k poly_e[k] t^k, t = (lambda - theta) / delta
   double poly_e[kPolyMax + 1];
@@ -328,6 +329,7 @@ template <typename T>
 __device__ __forceinline__ bool krylov_start(const GArgs<T>& A, GDev* d) {
   d->j = 0;
   d->ja = 0;
+  d->arn_stop = 0;
   d->rho = d->rho0;
   kry_gv(A)[0] = d->rho0;
   kry_sj(A)[0] = d->rho0 > 0.0 ? 1.0 / d->rho0 : 0.0;
@@ -745,7 +747,10 @@ __global__ void __launch_bounds__(kThreads) kg_accept(GArgs<T> A) {
 //   kg_arn_apply  Z_ja = U_ja - dt/2 J(x) U_ja  (A U_ja; the tangent-linear product is
 //                 linear)
 //   kg_arn_dots   <Z_ja, U_i> (i <= ja) over the interior entries (||U_ja||^2 comes
-//                 with the orthogonalisation).
+//                 with the orthogonalisation; kg_arn_check, between the
+//                 orthogonalisation and the product, completes column ja - 1
+//                 from it and stops the solve before the products when it
+//                 has converged).
 // The basis stays unnormalised (v_i = s_i U_i, s_i = 1 / ||U_i||): with
 // gam_i = s_i^2 <Z_{ja-1}, U_i>, U_ja is the classical Gram-Schmidt remainder of
 // A v_{ja-1}, so ||U_ja|| = h_{ja,ja-1} stays of the order of ||A|| (without the
@@ -753,10 +758,12 @@ __global__ void __launch_bounds__(kThreads) kg_accept(GArgs<T> A) {
 // leave the FP32 range within a few dozen iterations of a stiff system).
 // The partials are added in a fixed order (the last block of each group of 32
 // blocks sums its group, the last group sums the groups), and that last block
-// completes Hessenberg column ja-1 (norm, Givens rotation, residual estimate
-// and the stop test of tgcr.py:125, 141-142) and, when the iteration goes on,
-// stores column ja and the next coefficients.  A
-// solve of m iterations takes m + 1 steps; the last product is not used.
+// stores column ja and the next coefficients.  Column ja-1 (norm, Givens
+// rotation, residual estimate and the stop test of tgcr.py:125, 141-142) is
+// completed earlier in the step, by kg_arn_check right after the
+// orthogonalisation: a solve of m iterations stops in the check of step m,
+// before that step's polynomial steps, product and projections, which then
+// return at once.
 //
 // The vectors live on the full grid with their face values, and the boundary
 // procedure is linear for directions, so kg_arn_orth combines every entry
@@ -764,45 +771,59 @@ __global__ void __launch_bounds__(kThreads) kg_accept(GArgs<T> A) {
 // the raw values and zeroes the dead links of the stencil's neighbours (normal
 // links on plane N-1, hole links) on the fly.
 
-// Column bookkeeping of launch ja (thread 0 of the last block).  S[i] = <Z_ja, U_i>, S[ja+1] = ||U_ja||^2.
+// Completion of Hessenberg column ja - 1 at Arnoldi step ja > 0, from
+// un2 = ||U_ja||^2 (thread 0 of kg_arn_check, before the step's products):
+// h_{ja, ja-1} = ||U_ja||, the Givens rotation, the residual estimate and the
+// stop test of tgcr.py:125, 141-142.  When the solve stops here the Krylov
+// loop ends and the step's products are marked skipped (arn_stop).
+template <typename T>
+__device__ void arn_complete(const GArgs<T>& A, GDev* d, int ja, double un2) {
+  if (!isfinite(un2)) { abort_all(A, GS_NONFINITE); return; }
+  double* sj = kry_sj(A);
+  const int jc = ja;                                   // columns complete after this step
+  double* gv = kry_gv(A);
+  double* cs = kry_cs(A);
+  double* sn = kry_sn(A);
+  double* col = kry_H(A) + (long)(jc - 1) * (A.kmax + 1);
+  const double un = sqrt(un2);
+  const double hn = un;                                // h_{jc, jc-1} = ||A v - sum h v|| = ||U_jc||
+  sj[jc] = un > 0.0 ? 1.0 / un : 0.0;
+  d->jvp_evals += 1 + A.poly_deg;
+  col[jc] = hn;
+  for (int i = 0; i + 1 < jc; ++i) {
+    double a = col[i], b = col[i + 1];
+    col[i] = cs[i] * a + sn[i] * b;
+    col[i + 1] = -sn[i] * a + cs[i] * b;
+  }
+  double a = col[jc - 1], b = col[jc];
+  double r = hypot(a, b);
+  double c = r > 0.0 ? a / r : 1.0, sv = r > 0.0 ? b / r : 0.0;
+  cs[jc - 1] = c;
+  sn[jc - 1] = sv;
+  col[jc - 1] = r;
+  col[jc] = 0.0;
+  gv[jc] = -sv * gv[jc - 1];
+  gv[jc - 1] = c * gv[jc - 1];
+  d->rho = fabs(gv[jc]);
+  d->j = jc;
+  bool cont = hn > 0.0 && d->rho / d->rho0 > d->tol_gcr && jc < d->krylov_max_iter;
+  if (cont && jc + 1 > A.kmax) { abort_all(A, GS_KMAX); return; }
+  if (!cont) {
+    d->arn_stop = 1;
+    cudaGraphSetConditional(A.h_krylov, 0);
+  }
+}
+
+// Column bookkeeping of launch ja (thread 0 of the last block), after
+// kg_arn_check has completed column ja - 1: S[i] = <Z_ja, U_i> gives column
+// ja's projections and the next orthogonalisation coefficients.
 template <typename T>
 __device__ void arn_finish(const GArgs<T>& A, GDev* d, int ja, const double* S) {
   if (++d->watchdog > d->watchdog_cap) { abort_all(A, GS_CAP); return; }
   double* sj = kry_sj(A);
   double* gam = kry_gam(A);
-  for (int i = 0; i <= ja + 1; ++i)
+  for (int i = 0; i <= ja; ++i)
     if (!isfinite(S[i])) { abort_all(A, GS_NONFINITE); return; }
-  if (ja > 0) {
-    const int jc = ja;                                   // columns complete after this launch
-    double* gv = kry_gv(A);
-    double* cs = kry_cs(A);
-    double* sn = kry_sn(A);
-    double* col = kry_H(A) + (long)(jc - 1) * (A.kmax + 1);
-    const double un = sqrt(S[ja + 1]);
-    const double hn = un;                                // h_{jc, jc-1} = ||A v - sum h v|| = ||U_jc||
-    sj[jc] = un > 0.0 ? 1.0 / un : 0.0;
-    d->jvp_evals += 1 + A.poly_deg;
-    col[jc] = hn;
-    for (int i = 0; i + 1 < jc; ++i) {
-      double a = col[i], b = col[i + 1];
-      col[i] = cs[i] * a + sn[i] * b;
-      col[i + 1] = -sn[i] * a + cs[i] * b;
-    }
-    double a = col[jc - 1], b = col[jc];
-    double r = hypot(a, b);
-    double c = r > 0.0 ? a / r : 1.0, sv = r > 0.0 ? b / r : 0.0;
-    cs[jc - 1] = c;
-    sn[jc - 1] = sv;
-    col[jc - 1] = r;
-    col[jc] = 0.0;
-    gv[jc] = -sv * gv[jc - 1];
-    gv[jc - 1] = c * gv[jc - 1];
-    d->rho = fabs(gv[jc]);
-    d->j = jc;
-    bool cont = hn > 0.0 && d->rho / d->rho0 > d->tol_gcr && jc < d->krylov_max_iter;
-    if (cont && jc + 1 > A.kmax) { abort_all(A, GS_KMAX); return; }
-    if (!cont) { cudaGraphSetConditional(A.h_krylov, 0); return; }
-  }
   double* colj = kry_H(A) + (long)ja * (A.kmax + 1);
   for (int i = 0; i <= ja; ++i) {
     colj[i] = sj[ja] * sj[i] * S[i];
@@ -945,6 +966,7 @@ template <typename T, bool D3>
 __global__ void __launch_bounds__(kThreads, 3) kg_arn_apply(GArgs<T> A) {
   GDev* d = A.dev;
   if (!gdev_ok(d)) return;
+  if (d->arn_stop && !A.standalone) return;   // the solve stopped at this step's check
   kt_begin(d, KT_ARN_APPLY);
   constexpr int NC = D3 ? 5 : 4;
   const Grid& g = A.g;
@@ -1042,6 +1064,7 @@ __global__ void __launch_bounds__(kThreads, 3) kg_arn_poly(GArgs<T> A) {
   GDev* d = A.dev;
   if (!gdev_ok(d)) return;
   if (A.pmode && d->newton_failed) return;
+  if (!A.pmode && d->arn_stop && !A.standalone) return;   // the solve stopped at this step's check
   kt_begin(d, KT_ARN_APPLY);
   constexpr int NC = D3 ? 5 : 4;
   const Grid& g = A.g;
@@ -1141,11 +1164,9 @@ __device__ bool arn_fold_groups(const GArgs<T>& A, const double* part, int nb, i
 }
 
 // Final fold (whole block of the last group): S[s] = sum over the ng group
-// partials for s <= ja, S[ja + 1] = ||U_ja||^2 from the orthogonalisation's
-// nblk_orth partials (ja > 0), all in a fixed order.
+// partials for s <= ja, in a fixed order.
 template <typename T>
 __device__ void arn_fold_final(const GArgs<T>& A, int ng, int ja, double* S) {
-  __shared__ double ow[kWarps];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int s2 = warp; s2 <= ja; s2 += kWarps) {
     double a = 0.0;
@@ -1153,18 +1174,31 @@ __device__ void arn_fold_final(const GArgs<T>& A, int ng, int ja, double* S) {
     a = warp_sum(a);
     if (lane == 0) S[s2] = a;
   }
+  __syncthreads();
+}
+
+// Stop test of Arnoldi step ja before its products (one block): folds
+// ||U_ja||^2 from the orthogonalisation's nblk_orth partials in a fixed order
+// and completes column ja - 1 (arn_complete).  A solve of m iterations runs m
+// full steps and stops in the check of step m, so no product goes unused.
+template <typename T>
+__global__ void kg_arn_check(GArgs<T> A) {
+  __shared__ double ow[kWarps];
+  GDev* d = A.dev;
+  if (!gdev_ok(d)) return;
+  const int ja = d->ja;
+  if (ja == 0) return;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   double o = 0.0;
-  if (ja > 0)
-    for (int bb = threadIdx.x; bb < A.nblk_orth; bb += kThreads) o += __ldcg(A.part_orth + bb);
+  for (int bb = threadIdx.x; bb < A.nblk_orth; bb += kThreads) o += __ldcg(A.part_orth + bb);
   o = warp_sum(o);
   if (lane == 0) ow[warp] = o;
   __syncthreads();
-  if (threadIdx.x == 0) {
-    double a = 0.0;
-    for (int w = 0; w < kWarps; ++w) a += ow[w];
-    S[ja + 1] = a;
-  }
-  __syncthreads();
+  if (threadIdx.x != 0) return;
+  double un2 = 0.0;
+  for (int w = 0; w < kWarps; ++w) un2 += ow[w];
+  arn_complete(A, d, ja, un2);
+  if (d->arn_stop) kt_fold(d, KT_ARN_ORTH);
 }
 
 // Projections <Z_ja, U_i> (i <= ja) over the interior entries (imask) in one
@@ -1181,6 +1215,7 @@ __global__ void __launch_bounds__(kThreads, 4) kg_arn_dots(GArgs<T> A) {
     if (blockIdx.x == 0 && threadIdx.x == 0) abort_all(A, d->status);
     return;
   }
+  if (d->arn_stop && !A.standalone) return;   // the solve stopped at this step's check
   kt_begin(d, KT_ARN_DOTS);
   extern __shared__ double red[];              // [kWarps][ja + 2]
   const int ja = d->ja;
@@ -1279,6 +1314,7 @@ __global__ void __launch_bounds__(kThreads, 3) kg_arn_apply_dots(GArgs<T> A) {
     if (blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x == 0) abort_all(A, d->status);
     return;
   }
+  if (d->arn_stop && !A.standalone) return;   // the solve stopped at this step's check
   kt_begin(d, KT_ARN_APPLY);
   constexpr int NC = D3 ? 5 : 4;
   constexpr int VC = ProdChunk<T>::VC;

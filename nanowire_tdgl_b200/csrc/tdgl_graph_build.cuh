@@ -102,6 +102,7 @@ cudaError_t build_trap_graph(GArgs<T> A, cudaGraph_t* out_graph, cudaGraphExec_t
     TDGL_GCK(cudaFuncSetAttribute((const void*)kg_arn_orth<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smo));
     TDGL_GCK(cudaFuncSetAttribute((const void*)kg_arn_dots<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smd));
     TDGL_GCK(ck.kernel((const void*)kg_arn_orth<T>, A.nblk_orth, kThreads, smo, A));
+    TDGL_GCK(ck.kernel((const void*)kg_arn_check<T>, 1, kThreads, 0, A));
     for (int k = A.poly_deg - 1; k >= 0; --k) {   // p(A) U_ja into PW[0]
       GArgs<T> P = A;
       P.pstep = k;
