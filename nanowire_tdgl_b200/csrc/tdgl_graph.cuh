@@ -180,16 +180,19 @@ struct NbE {
 };
 // NbE through the read-only data path (ld.global.nc): for buffers that no
 // thread of the launch writes (the Arnoldi product's linearisation copy).
+// Neighbour offsets are 32-bit from the node's address (a component block of
+// the full grid stays far below 2^31 entries / 4), so each read is one
+// address computation from a loop-invariant base.
 template <typename T>
 struct NbEro {
   const T* __restrict__ E; long npf; long m; int mj, mk;
   __device__ __forceinline__ void psi(int di, int dj, int dk, T& re, T& im) const {
-    long e = m + di + (long)dj * mj + (long)dk * mk;
-    re = __ldg(E + e);
-    im = __ldg(E + npf + e);
+    const T* p = E + m + (di + dj * mj + dk * mk);
+    re = __ldg(p);
+    im = __ldg(p + (int)npf);
   }
   __device__ __forceinline__ T phi(int a, int di, int dj, int dk) const {
-    return __ldg(E + (2 + a) * npf + m + di + (long)dj * mj + (long)dk * mk);
+    return __ldg(E + m + ((2 + a) * (int)npf + di + dj * mj + dk * mk));
   }
 };
 // E1 + s * E2 (finite-difference point x + eps v in effective form: the boundary
@@ -884,14 +887,14 @@ template <typename T>
 struct NbMk {
   const T* __restrict__ E; long npf; long m; int mj, mk; uint32_t dm; NbM<T> slow;
   __device__ __forceinline__ void psi(int di, int dj, int dk, T& re, T& im) const {
-    long e = m + di + (long)dj * mj + (long)dk * mk;
-    re = __ldg(E + e);
-    im = __ldg(E + npf + e);
+    const T* p = E + m + (di + dj * mj + dk * mk);
+    re = __ldg(p);
+    im = __ldg(p + (int)npf);
   }
   __device__ __forceinline__ T phi(int a, int di, int dj, int dk) const {
     const int b = dead_bit(a, di, dj, dk);
     if (b < 0) return slow.phi(a, di, dj, dk);
-    const T v = __ldg(E + (2 + a) * npf + m + di + (long)dj * mj + (long)dk * mk);
+    const T v = __ldg(E + m + ((2 + a) * (int)npf + di + dj * mj + dk * mk));
     return ((dm >> b) & 1u) ? T(0) : v;
   }
 };
