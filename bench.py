@@ -114,10 +114,10 @@ def algorithmic_bytes(n_int: int, precision: str, st: dict, poly_deg: int = 0) -
                                                   sum_k (2(k-1) + 8) SK = (m^2 + 7 m) SK
       Newton residual, norms, x += dx            7 S64 per Newton iteration
     This is the per-stage model of the reference's GCR form.  The GMRES form
-    run here moves, per solve of m iterations, sum_{j=0..m} (2 j + 7) SK =
-    (m^2 + 8 m + 7) SK (orthogonalisation j + 2 vectors, product 3,
-    projections j + 2; one more step than iterations), within a few percent of
-    the model at m ~ 25, and the measured DRAM traffic is 0.93 x the model.
+    run here moves, per solve of m iterations, sum_{j=0..m-1} (2 j + 7) SK
+    (orthogonalisation j + 2 vectors, product 3, projections j + 2) plus the
+    last step's orthogonalisation (its products are skipped once its stop
+    check has ended the solve), within a few percent of the model at m ~ 25.
     With the polynomial preconditioner of degree d, every Arnoldi column and
     every Newton correction takes d more stencil launches (counted in
     jvp_evals, 3 SK + F each) that also read the vector they precondition
