@@ -656,13 +656,16 @@ def run_batched(a, rank: int = 0, world: int = 1):
                        "interior_nodes_total": sum(n_nodes), "interior_nodes_min": min(n_nodes),
                        "interior_nodes_max": max(n_nodes), "holes_total": sum(q[3] for q in desc),
                        "streams": len(bt.streams), "kmax": a.kmax},
-            "autotune_ms_per_2_steps": {f"{k[0]} nodes/thread, {'one' if k[1] else 'two'} kernel(s)": v
+            "autotune_ms_per_2_steps": {f"{k[0]} nodes/thread, {'one' if k[1] else 'two'} kernel(s)"
+                                        + (f", degree {k[2]}" if len(k) > 2 else ""): v
                                         for k, v in tune.items()},
-            "shape": {"nodes_per_thread": bt.best[0], "fused_product_projections": bool(bt.best[1])},
+            "shape": {"nodes_per_thread": bt.best[0], "fused_product_projections": bool(bt.best[1]),
+                      "poly_degree": bt.best[2] if len(bt.best) > 2 else None},
             "counters": cnt,
             "max_rel_l2_psi2_batched_vs_looping": max_over_ranks(max(rel), dist, "cuda"),
-            "note": "batched and looping differ only in launch shapes (reduction partitions); at equal shapes "
-                    "the results are bit-identical",
+            "note": "batched and looping differ in launch shapes (reduction partitions) and, when the autotuner "
+                    "picks another degree than the default 3, in the preconditioner (converged states agree to "
+                    "the Newton tolerance); at equal shapes and degree the results are bit-identical",
             "device_memory_in_use_gb": (total - free) / 1e9,
             "clocks": clk}
 
