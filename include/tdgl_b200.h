@@ -246,7 +246,7 @@ int tdgl_ctx_set_blocks(tdgl_ctx* ctx, int32_t stream_blocks, int32_t krylov_blo
  * [1 - dt/2, 1 + dt/2 rho], rho a Gershgorin bound of J; the Newton
  * correction is p(A) times the Krylov combination, so the stop test and the
  * solution are those of the unpreconditioned system.  0 turns it off, -1
- * restores the default (3, or TDGL_POLY_DEGREE).  The finite-difference
+ * restores the default (5, or TDGL_POLY_DEGREE).  The finite-difference
  * (reference) form never uses it.  The graph is rebuilt at the next launch;
  * TDGL_EINVAL while a launch is pending.  No reference counterpart (the
  * reference's GCR is unpreconditioned). */

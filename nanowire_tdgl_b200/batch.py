@@ -183,7 +183,7 @@ class BatchedTrapezoidal:
         the fastest.  States, clocks and counters are restored.  Returns
         {candidate: ms}.  (Stiffer instances, larger kappa^2 dt / h^2, gain
         from the higher degree: on the 64-instance workload degree 5 stepped
-        9 % faster than the default 3.)"""
+        9 % faster than degree 3.)"""
         snap = self.snapshot()
         times = {}
         for cand in candidates:

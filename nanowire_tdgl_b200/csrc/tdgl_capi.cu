@@ -36,7 +36,7 @@ static constexpr long kProfLen = 64 + 2 * 1024;
 // upper bound of the step graph's blocks per SM (its partial-sum buffers are sized for it)
 static constexpr int kMaxBlocksPerSm = 8;
 // default degree of the polynomial preconditioner (analytic-product GMRES)
-static constexpr int kPolyDefault = 3;
+static constexpr int kPolyDefault = 5;
 
 namespace {
 
