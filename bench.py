@@ -41,6 +41,7 @@ WORKLOAD = dict(Nx=128, Ny=128, Nz=32, h=0.5, kappa=2.0, Bz=0.5, hole=[(24, 24),
 WORKLOAD_NAME = ("trapezoidal step, 128x128x32-cell film (499,999 interior nodes), 32x32-node hole through "
                  "all planes, h=0.5, kappa=2, Bz=0.5, dt=0.1, Newton tol_f 1e-8 / tol_dx 1e-3, GCR tol 1e-6")
 HBM_FALLBACK_GBS = 6650.0
+WORKLOAD_N_INTERIOR = 127 * 127 * 31
 # DRAM bytes per algorithmic byte of the GMRES step graph on the 128x128x32
 # workload (degree-3 preconditioner), from a graph-level ncu capture of a
 # 2-step launch: 6.49 GB DRAM against 15.0 GB algorithmic.  The preconditioned
@@ -312,7 +313,9 @@ def run_ours(a, rank, world):
                    "preconditioner": f"Chebyshev polynomial, degree {poly_deg}" if poly_deg else "none",
                    "n_interior": n_int,
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                   "l2": "inputs larger than L2: Krylov basis of ~2x26 state vectors (>0.5 GB) per solve"},
+                   "l2": ("inputs larger than L2: each step touches ~0.3 GB (FP64 state, iterate, gamma and f, "
+                          "their full-grid copies, the FP32 linearisation copy, Krylov basis and preconditioner "
+                          "buffers) against the 126 MB L2; no flush between steps")},
         "node_updates_per_s": value * n_int,
         "gpu_launches": graph_launches(st, jvp, poly_deg) if a.krylov == "gmres" else 1,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
@@ -350,6 +353,12 @@ def run_ours(a, rank, world):
         out["speedup_vs_fp64"] = {mode: out["value"] / world / v["value"] for mode, v in out["fp64"].items()}
         out["rel_l2_psi2_vs_fp64"] = rel
         out["max_abs_psi2_vs_fp64"] = float((p2m - p2d).abs().max())
+    # the state after step 1 from the seeded state (t = 0), for the comparison
+    # with the oracle's step 1 (computed by the CPU-baseline leg)
+    x1 = g.pack(x0)
+    rc, _, _, _ = g.trap_run(x1, 0.0, w["dt"], 1, opts, fld)
+    if rc == 0:
+        out["_x1"] = g.unpack(x1).cpu().numpy()
     # end to end through the public API: host numpy state in, every step's state back to the host
     if not a.no_e2e:
         sched = tb.FieldSchedule(dev.applied_field, p, dev.idx, w["t_stop"])
@@ -378,8 +387,9 @@ def run_ours(a, rank, world):
     return out
 
 
-def cpu_oracle_steps(max_steps: int, budget_s: float, threads: int):
-    """Time the oracle's trapezoidal steps on the host (bounded by budget_s)."""
+def cpu_oracle_steps(max_steps: int, budget_s: float, threads: int, want_state: bool = False):
+    """Time the oracle's trapezoidal steps on the host (bounded by budget_s);
+    with want_state, also return the state after the first step."""
     from threadpoolctl import threadpool_limits
     from oracle import tdgl_oracle as orc
     dev, x0 = build_device()
@@ -389,6 +399,7 @@ def cpu_oracle_steps(max_steps: int, budget_s: float, threads: int):
     X = x0
     t = 0.0
     done = 0
+    first = None
     t0 = time.perf_counter()
     with threadpool_limits(limits=threads):
         while done < max_steps:
@@ -397,9 +408,13 @@ def cpu_oracle_steps(max_steps: int, budget_s: float, threads: int):
                                           max_steps=1)
             X, t = hist[:, -1], times[-1]
             done += 1
+            if done == 1:
+                first = X.copy()
             if time.perf_counter() - t0 > budget_s:
                 break
     el = time.perf_counter() - t0
+    if want_state:
+        return done, el, first
     return done, el
 
 
@@ -786,12 +801,21 @@ def main():
     finally:
         if world > 1:
             torch.distributed.destroy_process_group()
+    x1 = out.pop("_x1", None)
     if rank == 0:
         if world == 1 and not a.no_cpu_baseline:
-            done, el = cpu_oracle_steps(1, a.cpu_budget_s, 1)
+            done, el, xo = cpu_oracle_steps(1, a.cpu_budget_s, 1, want_state=True)
             out["cpu_baseline"] = {"value": done / el, "unit": "steps/s", "cores": 1, "kind": "port",
                                    "sample": f"{done} trapezoidal step(s) from the seeded state (step 1), numpy "
                                              "oracle restating the reference algorithm, 1 thread"}
+            if x1 is not None and xo is not None:
+                n = WORKLOAD_N_INTERIOR
+                p2, p2o = np.abs(x1[:n]) ** 2, np.abs(xo[:n]) ** 2
+                out["rel_l2_psi2_vs_oracle"] = float(np.linalg.norm(p2 - p2o) / np.linalg.norm(p2o))
+                out["max_abs_vs_oracle"] = float(np.max(np.abs(x1 - xo)))
+                out["vs_oracle_note"] = (f"state after step 1 from the seeded state: this run's {a.precision} "
+                                         "stepper against the oracle's FP64 finite-difference GCR step (same "
+                                         "tolerances); max_abs over all state entries")
         print(json.dumps(out), flush=True)
     return 0
 

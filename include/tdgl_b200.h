@@ -54,7 +54,10 @@ typedef enum tdgl_precision {
 
 typedef enum tdgl_jvp_mode {
   TDGL_JVP_FD = 0,       /* (f(x + eps p) - f(x)) / eps, eps = eps_mf (1 + |x|) / |p| (tgcr.py:129-133); FP64 only */
-  TDGL_JVP_ANALYTIC = 1  /* exact tangent-linear RHS */
+  TDGL_JVP_ANALYTIC = 1, /* exact tangent-linear RHS */
+  TDGL_JVP_KRYLOV = 2    /* tdgl_jvp only: the exact product as the context's analytic-product
+                            Krylov solves compute it (its Krylov precision, FP32 for TDGL_MIXED;
+                            the step graph's stencil kernel on the full-grid layout) */
 } tdgl_jvp_mode;
 
 typedef enum tdgl_krylov {
@@ -163,7 +166,11 @@ int tdgl_vjp(tdgl_ctx* ctx, const double* x_dev, const double* v_dev, double Bx,
 int tdgl_eval_f(tdgl_ctx* ctx, const double* x_ref, double* f_ref, double Bx, double By, double Bz,
                 tdgl_stream_t stream);
 /* ap = p - dt/2 J(x) p in the device layout (the A*p of tgcr_matrix_free_trap,
- * src/tdgl3d/solvers/tgcr.py:129-133).  mode FD uses eps = eps_mf (1+|x|)/|p|. */
+ * src/tdgl3d/solvers/tgcr.py:129-133).  mode FD uses eps = eps_mf (1+|x|)/|p|.
+ * mode TDGL_JVP_KRYLOV runs the stepper's own product kernel in the context's
+ * Krylov precision on its stepping workspace and blocks until the stream has
+ * passed it (TDGL_EINVAL while a tdgl_trap_launch is uncollected;
+ * TDGL_ETIMEOUT when a bounded wait of the kernel ran out). */
 int tdgl_jvp(tdgl_ctx* ctx, const double* x_dev, const double* p_dev, double* ap_dev, double dt, int32_t mode,
              double eps_mf, double Bx, double By, double Bz, tdgl_stream_t stream);
 /* Observables at interior nodes in reference order (n_interior doubles each):
@@ -240,6 +247,16 @@ int tdgl_trap_collect(tdgl_ctx* ctx, double* t, double* dt_cur, tdgl_stats* stat
  * (small instances run concurrently on few blocks each); the graph is rebuilt
  * at the next launch.  No reference counterpart. */
 int tdgl_ctx_set_blocks(tdgl_ctx* ctx, int32_t stream_blocks, int32_t krylov_blocks, int32_t fused);
+/* Limits of the context's device-side waits and loops (no reference
+ * counterpart; the reference runs on one host thread and has none):
+ * wait_ns bounds every single wait inside a kernel (the persistent kernel's
+ * grid barrier, the staged-copy waits of the TMA-staged stencil), after which
+ * the kernel stops and the call returns TDGL_ETIMEOUT; loop_cap bounds the
+ * conditional-loop iterations of one step-graph launch, after which the
+ * launch stops and the call returns TDGL_ETIMEOUT.  Values <= 0 restore the
+ * defaults (5 s; a cap derived from max_steps, newton_max_iter and kmax).
+ * The context stays usable after either limit has run out. */
+int tdgl_ctx_set_limits(tdgl_ctx* ctx, int64_t wait_ns, int64_t loop_cap);
 /* Degree (0 to 8) of the polynomial right preconditioner of the GMRES solves
  * with analytic Jacobian products: GMRES runs on A p(A), A = I - dt/2 J,
  * p the Chebyshev-iteration polynomial of that degree for the interval

@@ -16,7 +16,7 @@ LIB_PATH = os.path.join(HERE, "libtdgl_b200.so")
 TDGL_OK, TDGL_ENOCONV, TDGL_EDTMIN, TDGL_EKMAX, TDGL_ENONFINITE, TDGL_ETIMEOUT, TDGL_EINVAL, TDGL_ECUDA, \
     TDGL_ENOMEM = range(9)
 TDGL_FP64, TDGL_MIXED = 0, 1
-TDGL_JVP_FD, TDGL_JVP_ANALYTIC = 0, 1
+TDGL_JVP_FD, TDGL_JVP_ANALYTIC, TDGL_JVP_KRYLOV = 0, 1, 2
 TDGL_KRYLOV_GMRES, TDGL_KRYLOV_GCR = 0, 1
 
 
@@ -88,6 +88,7 @@ SIGNATURES = {
     "tdgl_trap_collect": (C.c_int, [_P, C.POINTER(_D), C.POINTER(_D), C.POINTER(Stats)]),
     "tdgl_ctx_set_blocks": (C.c_int, [_P, _I, _I, _I]),
     "tdgl_ctx_set_poly": (C.c_int, [_P, _I]),
+    "tdgl_ctx_set_limits": (C.c_int, [_P, C.c_int64, C.c_int64]),
     "tdgl_ctx_poly_degree": (C.c_int32, [_P]),
     "tdgl_euler_run": (C.c_int, [_P, _P, C.POINTER(_D), _D, _D, _I, C.POINTER(Field), _P]),
     "tdgl_vjp": (C.c_int, [_P, _P, _P, _D, _D, _D, _P, _P, _P, _P, _P]),

@@ -18,6 +18,9 @@
 #include "tdgl_adjoint.cuh"
 #include "tdgl_analysis.cuh"
 #include "tdgl_adjoint_graph.cuh"
+#include "tdgl_tl.cuh"
+
+#include <cudaTypedefs.h>
 
 using namespace tdgl;
 
@@ -26,9 +29,13 @@ cudaError_t stepper_occupancy_f32(size_t smem, int* occ);
 cudaError_t stepper_occupancy_f64(size_t smem, int* occ);
 cudaError_t stepper_launch_f32(StepArgs<float> A, int blocks, size_t smem, cudaStream_t s);
 cudaError_t stepper_launch_f64(StepArgs<double> A, int blocks, size_t smem, cudaStream_t s);
-cudaError_t graph_build_f32(const GArgs<float>& A, cudaGraph_t* graph, cudaGraphExec_t* exec);
+cudaError_t graph_build_f32(const GArgs<float>& A, const TlMaps* tm, int chunks, cudaGraph_t* graph,
+                            cudaGraphExec_t* exec);
 cudaError_t graph_build_f64(const GArgs<double>& A, cudaGraph_t* graph, cudaGraphExec_t* exec);
-cudaError_t arnoldi_probe_f32(const GArgs<float>& A, int launches, int kernels, cudaStream_t s);
+cudaError_t arnoldi_probe_f32(const GArgs<float>& A, const TlMaps* tm, int chunks, int launches, int kernels,
+                              cudaStream_t s);
+cudaError_t product_f32(const GArgs<float>& A, const TlMaps* tm, int chunks, cudaStream_t s);
+cudaError_t product_f64(const GArgs<double>& A, cudaStream_t s);
 cudaError_t arnoldi_probe_f64(const GArgs<double>& A, int launches, int kernels, cudaStream_t s);
 }  // namespace tdgl
 
@@ -37,6 +44,8 @@ static constexpr long kProfLen = 64 + 2 * 1024;
 static constexpr int kMaxBlocksPerSm = 8;
 // default degree of the polynomial preconditioner (analytic-product GMRES)
 static constexpr int kPolyDefault = 5;
+// default limit of one bounded device wait (grid barrier, staged-copy mbarrier)
+static constexpr unsigned long long kWaitDefaultNs = 5000000000ull;
 
 namespace {
 
@@ -140,6 +149,16 @@ struct tdgl_ctx {
   bool pending = false, pending_noop = false;   // an uncollected tdgl_trap_launch
   uint8_t* imask = nullptr;
   uint32_t* deadmask = nullptr;   // per interior node: dead links read by the Arnoldi product
+  uint8_t* ldead = nullptr;       // per full-grid node: its dead links (TMA-staged stencil)
+  // TMA-staged tangent-linear stencil (FP32 vectors, 3-D grids): tensor maps of
+  // the staged vectors and the z-chunks per tile column
+  TlMaps tlm{};
+  bool tl_on = false;
+  int tl_chunks = 0;
+  // limits of the device's bounded waits and of the graph's loop iterations
+  // (tdgl_ctx_set_limits; 0: the defaults)
+  unsigned long long wait_ns = kWaitDefaultNs;
+  long long watchdog_req = 0;
   // adjoint scratch (allocated on first use)
   double* vjp_part = nullptr;   // 3 x vjp blocks
   double* vjp_k2 = nullptr;     // n
@@ -376,9 +395,13 @@ __global__ void k_norm2(const double* __restrict__ v, long L, double* out) {
   }
 }
 
+static int krylov_product(tdgl_ctx* c, const double* x, const double* p, double* ap, double dt, double Bx,
+                          double By, double Bz, tdgl_stream_t s);
+
 extern "C" int tdgl_jvp(tdgl_ctx* c, const double* x, const double* p, double* ap, double dt, int32_t mode,
                         double eps_mf, double Bx, double By, double Bz, tdgl_stream_t s) {
   if (!c || !x || !p || !ap) return fail(TDGL_EINVAL, "null argument");
+  if (mode == TDGL_JVP_KRYLOV) return krylov_product(c, x, p, ap, dt, Bx, By, Bz, s);
   BTerms<double> b = bterms(c->g, Bx, By, Bz);
   if (mode == TDGL_JVP_ANALYTIC) {
     k_jvp_analytic<double><<<grid_1d(c, c->g.n), kThreads, 0, s>>>(c->g, x, p, ap, dt / 2.0, b);
@@ -497,7 +520,7 @@ static StepArgs<T> make_args(tdgl_ctx* c, double* x0, double* x1, double* G, dou
   A.sy.bar = c->bar;
   A.sy.err = c->err;
   A.sy.nslot_max = c->kmax + 4;
-  A.sy.timeout_ns = 5000000000ull;
+  A.sy.timeout_ns = c->wait_ns;
   A.ctl = c->ctl_dev;
   A.X[0] = x0;
   A.X[1] = x1;
@@ -696,6 +719,7 @@ static GArgs<T> make_gargs(tdgl_ctx* c) {
   A.arn_gy = c->arn_gy;
   A.apply_dots = c->apply_dots;
   A.deadmask = c->deadmask;
+  A.ldead = c->ldead;
   A.ntiles = c->ntiles;
   A.ngroups = c->ngroups;
   A.gpart = c->gpart;
@@ -734,6 +758,26 @@ static __global__ void k_deadmask(Grid g, uint32_t* __restrict__ mask) {
   }
 }
 
+// Dead links of every full-grid node (the rule of NbM::phi, stated per link
+// instead of per reading node): bit a when link a of the node is the normal
+// link on plane N-1 of axis a or a hole link.
+static __global__ void k_ldead(Grid g, long npf, uint8_t* __restrict__ out) {
+  const long dimx = g.is3d ? (long)g.mk * (g.Nz + 1) : (long)g.mk;
+  for (long m = blockIdx.x * (long)blockDim.x + threadIdx.x; m < npf; m += (long)gridDim.x * blockDim.x) {
+    uint8_t b = 0;
+    if (m < dimx) {
+      const int k = (int)(m / g.mk), r = (int)(m - (long)k * g.mk), j = r / g.mj, i = r - j * g.mj;
+      if (i <= g.Nx) {
+        b = g.lflags ? g.lflags[m] : (uint8_t)0;
+        if (i == g.Nx - 1) b |= 1u;
+        if (j == g.Ny - 1) b |= 2u;
+        if (g.is3d && k == g.Nz - 1) b |= 4u;
+      }
+    }
+    out[m] = b;
+  }
+}
+
 // Product and projections as one kernel or two: as set by tdgl_ctx_set_blocks,
 // else TDGL_ARN_APPLY_DOTS, else one kernel for FP64 vectors (the stencil's
 // arithmetic then hides more of the basis reads) and two for FP32 ones.
@@ -742,6 +786,51 @@ static int apply_dots_setting(const tdgl_ctx* c) {
   const char* e = std::getenv("TDGL_ARN_APPLY_DOTS");
   if (e && e[0]) return e[0] != '0';
   return c->precision == TDGL_FP64;
+}
+
+// Tensor maps of the TMA-staged stencil over the context's FP32 full-grid
+// vectors (3-D grids; TDGL_TMA=0 keeps the stencil that reads global memory):
+// dimensions (x, y, z, component[, vector]) with the padded row pitch, boxes
+// of 36 x 10 x 1 x 5 entries.  z-chunks per tile column: TDGL_TL_CHUNKS, else
+// as many as keep every block of the launch resident at once (3 per SM).
+static int setup_tl(tdgl_ctx* c) {
+  c->tl_on = false;
+  const Grid& g = c->g;
+  if (c->precision != TDGL_MIXED || !g.is3d) return TDGL_OK;
+  if (const char* e = std::getenv("TDGL_TMA"))
+    if (e[0] == '0') return TDGL_OK;
+  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  if (!encode) {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    cudaError_t e = cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &fn, 12000, cudaEnableDefault, &q);
+    if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !fn)
+      return fail(TDGL_ECUDA, "cuTensorMapEncodeTiled is not available from the driver");
+    encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+  }
+  const cuuint64_t fs = sizeof(float);
+  const cuuint64_t dims[5] = {(cuuint64_t)g.mj, (cuuint64_t)g.Ny + 1, (cuuint64_t)g.Nz + 1, (cuuint64_t)kTlComp,
+                              (cuuint64_t)c->kmax + 1};
+  const cuuint64_t strides[4] = {(cuuint64_t)g.mj * fs, (cuuint64_t)g.mk * fs, (cuuint64_t)c->npf * fs,
+                                 (cuuint64_t)kTlComp * (cuuint64_t)c->npf * fs};
+  const cuuint32_t box[5] = {(cuuint32_t)kTlBoxX, (cuuint32_t)kTlBoxY, 1u, (cuuint32_t)kTlComp, 1u};
+  const cuuint32_t es[5] = {1u, 1u, 1u, 1u, 1u};
+  if (g.ncomp != kTlComp || g.mj % 4 || c->npf % 4) return fail(TDGL_ECUDA, "full-grid layout not TMA-aligned");
+  void* base[5] = {c->XLe, c->UB, c->PW[0], c->PW[1], c->PC};
+  for (int t = 0; t < 5; ++t) {
+    const cuuint32_t rank = t == TM_UB ? 5u : 4u;
+    CUresult r = encode(&c->tlm.m[t], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, rank, base[t], dims, strides, box, es,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(TDGL_ECUDA, "cuTensorMapEncodeTiled failed (code " + std::to_string((int)r) + ")");
+  }
+  const int tiles = c->arn_gx * c->arn_gy;
+  int ch = std::max(1, (c->num_sms * 3) / std::max(tiles, 1));
+  if (const char* e = std::getenv("TDGL_TL_CHUNKS"))
+    if (std::atoi(e) > 0) ch = std::atoi(e);
+  c->tl_chunks = std::min(std::max(ch, 1), g.nz);
+  c->tl_on = true;
+  return TDGL_OK;
 }
 
 // Buffers of the three-kernel Arnoldi step (analytic products).
@@ -779,7 +868,10 @@ static int ensure_arnoldi_ws(tdgl_ctx* c) {
   if ((rc = ctx_alloc(c, (void**)&c->deadmask, sizeof(uint32_t) * (size_t)g.n))) return rc;
   k_deadmask<<<grid_1d(c, g.n), kThreads>>>(g, c->deadmask);
   TDGL_CUDA(cudaGetLastError());
-  return TDGL_OK;
+  if ((rc = ctx_alloc(c, (void**)&c->ldead, (size_t)c->npf))) return rc;
+  k_ldead<<<grid_1d(c, c->npf), kThreads>>>(g, c->npf, c->ldead);
+  TDGL_CUDA(cudaGetLastError());
+  return setup_tl(c);
 }
 
 // Block counts of the graph's grid kernels from the stream and Krylov settings:
@@ -841,7 +933,7 @@ static int ensure_graph(tdgl_ctx* c, int v) {
     GArgs<float> A = make_gargs<float>(c);
     A.fused = v;
     if (!v) A.poly_deg = 0;
-    e = graph_build_f32(A, &c->graph[v], &c->gexec[v]);
+    e = graph_build_f32(A, (v && c->tl_on) ? &c->tlm : nullptr, c->tl_chunks, &c->graph[v], &c->gexec[v]);
   } else {
     GArgs<double> A = make_gargs<double>(c);
     A.fused = v;
@@ -900,6 +992,8 @@ static int graph_launch(tdgl_ctx* c, double* x, double t0, double cur0, int32_t 
   // hard limit on loop iterations: every step may be retried down to dt_min
   // (at most ~12 cuts of dt/10 in double range) with full Newton / Krylov loops
   h.watchdog_cap = (long long)(max_steps + 1) * 40 * (o->newton_max_iter + 2) * (c->kmax + 3) + 1000;
+  if (c->watchdog_req > 0) h.watchdog_cap = c->watchdog_req;
+  h.wait_ns = c->wait_ns;
   h.prof_on = c->gprof ? 1 : 0;
   for (int k = 0; k < kKTypes; ++k) h.kt_start[k] = ~0ull;
   *noop = !(h.t < h.t_stop - 1e-14) || max_steps <= 0;
@@ -1137,6 +1231,72 @@ extern "C" int tdgl_euler_run(tdgl_ctx* c, double* x, double* t, double t_stop, 
   return TDGL_OK;
 }
 
+// ap = p - dt/2 J(x) p as the analytic-product Krylov solves compute it: x
+// staged as the linearisation copy (with the field's face offsets) and p as
+// basis vector 0, both on the full grid in the context's Krylov precision,
+// then the graph's product kernel (the TMA-staged one for FP32 3-D contexts)
+// and the interior entries back into the device layout.  Uses the stepping
+// workspace; blocks until the stream has passed the product, to report a
+// bounded wait that ran out.
+static int krylov_product(tdgl_ctx* c, const double* x, const double* p, double* ap, double dt, double Bx,
+                          double By, double Bz, tdgl_stream_t s) {
+  if (c->pending) return fail(TDGL_EINVAL, "a launch of this context has not been collected");
+  int rc;
+  if ((rc = ensure_graph(c, 1))) return rc;
+  const Grid& g = c->g;
+  const BTerms<double> b = bterms(g, Bx, By, Bz);
+  GDev& h = *c->gdev_host;
+  std::memset(&h, 0, sizeof(GDev));
+  h.dta = dt;
+  h.wait_ns = c->wait_ns;
+  for (int k = 0; k < kKTypes; ++k) h.kt_start[k] = ~0ull;
+  TDGL_CUDA(cudaMemcpyAsync(c->gdev, &h, sizeof(GDev), cudaMemcpyHostToDevice, s));
+  const int nb = grid_1d(c, g.n), nbp = grid_1d(c, g.npad);
+  cudaError_t e;
+  if (c->precision == TDGL_MIXED) {
+    GArgs<float> A = make_gargs<float>(c);
+    A.fused = 1;
+    A.standalone = 1;
+    A.poly_deg = 0;
+    if (g.is3d) {
+      kg_to_full<float, true, false><<<nb, kThreads, 0, s>>>(g, x, A.XLe, A.npf, b.czxy, b.cyzx, b.cxyz);
+      kg_to_full<float, true, true><<<nb, kThreads, 0, s>>>(g, p, A.UB, A.npf, 0.0, 0.0, 0.0);
+    } else {
+      kg_to_full<float, false, false><<<nb, kThreads, 0, s>>>(g, x, A.XLe, A.npf, b.czxy, b.cyzx, b.cxyz);
+      kg_to_full<float, false, true><<<nb, kThreads, 0, s>>>(g, p, A.UB, A.npf, 0.0, 0.0, 0.0);
+    }
+    e = product_f32(A, c->tl_on ? &c->tlm : nullptr, c->tl_chunks, s);
+    if (e == cudaSuccess) kg_from_full<float><<<nbp, kThreads, 0, s>>>(g, A.Zb[0], A.npf, ap);
+  } else {
+    GArgs<double> A = make_gargs<double>(c);
+    A.fused = 1;
+    A.standalone = 1;
+    A.poly_deg = 0;
+    if (g.is3d) {
+      kg_to_full<double, true, false><<<nb, kThreads, 0, s>>>(g, x, A.XLe, A.npf, b.czxy, b.cyzx, b.cxyz);
+      kg_to_full<double, true, true><<<nb, kThreads, 0, s>>>(g, p, A.UB, A.npf, 0.0, 0.0, 0.0);
+    } else {
+      kg_to_full<double, false, false><<<nb, kThreads, 0, s>>>(g, x, A.XLe, A.npf, b.czxy, b.cyzx, b.cxyz);
+      kg_to_full<double, false, true><<<nb, kThreads, 0, s>>>(g, p, A.UB, A.npf, 0.0, 0.0, 0.0);
+    }
+    e = product_f64(A, s);
+    if (e == cudaSuccess) kg_from_full<double><<<nbp, kThreads, 0, s>>>(g, A.Zb[0], A.npf, ap);
+  }
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(TDGL_ECUDA, std::string("Krylov product launch: ") + cudaGetErrorString(e));
+  TDGL_CUDA(cudaMemcpyAsync(&h.status, &c->gdev->status, sizeof(int), cudaMemcpyDeviceToHost, s));
+  TDGL_CUDA(cudaStreamSynchronize(s));
+  return graph_status(h.status);
+}
+
+extern "C" int tdgl_ctx_set_limits(tdgl_ctx* c, int64_t wait_ns, int64_t loop_cap) {
+  if (!c) return fail(TDGL_EINVAL, "null context");
+  if (c->pending) return fail(TDGL_EINVAL, "a launch of this context has not been collected");
+  c->wait_ns = wait_ns > 0 ? (unsigned long long)wait_ns : kWaitDefaultNs;
+  c->watchdog_req = loop_cap > 0 ? loop_cap : 0;
+  return TDGL_OK;
+}
+
 extern "C" int tdgl_arnoldi_probe(tdgl_ctx* c, int32_t ja, int32_t launches, int32_t kernels, tdgl_stream_t s) {
   if (!c || launches < 0) return fail(TDGL_EINVAL, "invalid argument");
   if (c->pending) return fail(TDGL_EINVAL, "a launch of this context has not been collected");
@@ -1149,7 +1309,7 @@ extern "C" int tdgl_arnoldi_probe(tdgl_ctx* c, int32_t ja, int32_t launches, int
     GArgs<float> A = make_gargs<float>(c);
     A.fused = 1;
     A.standalone = 1;
-    e = arnoldi_probe_f32(A, launches, kernels, s);
+    e = arnoldi_probe_f32(A, c->tl_on ? &c->tlm : nullptr, c->tl_chunks, launches, kernels, s);
   } else {
     GArgs<double> A = make_gargs<double>(c);
     A.fused = 1;

@@ -35,7 +35,14 @@ inline int build_geometry(const tdgl_grid_desc* gd, const tdgl_material_desc* md
   const bool d3 = Nz > 1;
   const long nx = Nx - 1, ny = Ny - 1, nz = d3 ? Nz - 1 : 1;
   const long n = nx * ny * nz;
-  const long mj = Nx + 1, mk = (Nx + 1) * (Ny + 1);
+  // Full-grid strides: the reference's (mjr, mkr: the index of its full-grid
+  // arrays, m = i + (Nx+1) j + (Nx+1)(Ny+1) k, src/tdgl3d/mesh/indices.py:46-55)
+  // for the input arrays, and the device's (mj, mk), whose rows are padded to a
+  // multiple of 4 entries so that every row of an FP32 full-grid vector starts
+  // on a 16-byte boundary (the row pitch a TMA tensor map requires).
+  const long mjr = Nx + 1, mkr = (Nx + 1) * (Ny + 1);
+  const long dimx_ref = d3 ? mkr * (Nz + 1) : mkr;
+  const long mj = round_up_l(Nx + 1, 4), mk = mj * (Ny + 1);
   const long dimx = d3 ? mk * (Nz + 1) : mk;
   if (n > (1L << 30) || dimx > (1L << 31) - 1) { err = "grid too large for 32-bit node indices"; return TDGL_EINVAL; }
   Grid& g = out.g;
@@ -67,8 +74,9 @@ inline int build_geometry(const tdgl_grid_desc* gd, const tdgl_material_desc* md
     int64_t nh = md ? md->n_hole_links[a] : 0;
     for (int64_t t = 0; t < nh; ++t) {
       int64_t m = hl[t];
-      if (m < 0 || m >= dimx) { err = "hole link index out of range"; return TDGL_EINVAL; }
-      lf[m] |= (uint8_t)(1u << a);
+      if (m < 0 || m >= dimx_ref) { err = "hole link index out of range"; return TDGL_EINVAL; }
+      const long i = m % mjr, q = m / mjr;
+      lf[i + mj * (q % (Ny + 1)) + mk * (q / (Ny + 1))] |= (uint8_t)(1u << a);
       any_hole = true;
     }
     const int64_t* hi = md ? md->hole_interior[a] : nullptr;
@@ -85,11 +93,11 @@ inline int build_geometry(const tdgl_grid_desc* gd, const tdgl_material_desc* md
   bool kappa_uniform = true;
   if (md && md->kappa_full) {
     k2.assign(n, 0.0);
-    kap0 = md->kappa_full[1 + mj + (d3 ? mk : 0)];
+    kap0 = md->kappa_full[1 + mjr + (d3 ? mkr : 0)];
     for (long k = (d3 ? 1 : 0); k <= (d3 ? Nz - 1 : 0); ++k)
       for (long j = 1; j <= ny; ++j)
         for (long i = 1; i <= nx; ++i) {
-          double kv = md->kappa_full[i + mj * j + mk * k];
+          double kv = md->kappa_full[i + mjr * j + mkr * k];
           k2[dev_of(i, j, k)] = kv * kv;
           if (kv != kap0) kappa_uniform = false;
         }

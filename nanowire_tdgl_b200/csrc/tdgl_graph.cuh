@@ -35,7 +35,9 @@
 
 namespace tdgl {
 
-enum GStatus : int { GS_OK = 0, GS_NOCONV = 1, GS_DTMIN = 2, GS_KMAX = 3, GS_NONFINITE = 4, GS_CAP = 5 };
+// GS_CAP: a loop ran past its watchdog count; GS_TIMEOUT: a bounded wait of a
+// kernel ran out (TMA-staged stencil).
+enum GStatus : int { GS_OK = 0, GS_NOCONV = 1, GS_DTMIN = 2, GS_KMAX = 3, GS_NONFINITE = 4, GS_CAP = 5, GS_TIMEOUT = 6 };
 
 constexpr int kKTypes = 16;   // slots of the per-kernel timers
 
@@ -52,6 +54,7 @@ struct GDev {
   double rho0, rho, xnorm, gnorm, dxnorm, eps;
   int steps, status, newton_k, newton_failed, accepted, j;
   long long watchdog, watchdog_cap;   // loop iterations of this launch and their hard limit
+  unsigned long long wait_ns;         // limit of one bounded wait inside a kernel
   // counters
   long long newton_iters, krylov_iters, krylov_sq, rhs_evals, jvp_evals, rejections;
   int max_krylov, krylov_last;
@@ -131,6 +134,8 @@ struct GArgs {
   // [(kmax + 1) x ntiles] in part_arn, group partials [(kmax + 1) x ngroups]
   int apply_dots;      // 1: kg_arn_apply_dots; 0: kg_arn_apply then kg_arn_dots
   const uint32_t* deadmask;   // per interior node: dead links among the product's neighbour reads
+  const uint8_t* ldead;       // per full-grid node: bit a set = its link a reads as zero (normal link on
+                              // plane N-1 of axis a, or a hole link); the rule NbM applies
   // adjoint solve (tdgl_adjoint_graph.cuh): linearisation state, right-hand
   // side, solution, J^T v scratch (device layout, L entries each)
   const double* ax;
@@ -272,6 +277,38 @@ __device__ __forceinline__ void write_eff(const Grid& g, T* E, long npf, int i, 
       if (k == g.Nz - 1) ghost(m - (long)(g.Nz - 1) * g.mk, 0.0, 0.0, tz);
       if (k == 1) ghost(m + (long)(g.Nz - 1) * g.mk, 0.0, 0.0, tz);
     }
+  }
+}
+
+// Full-grid copy in T of a device-layout FP64 vector x: the boundary
+// procedure's face values with the given field offsets; RAW: the nodes keep
+// their raw values (a Krylov direction), else they get the procedure too (a
+// linearisation state).
+template <typename T, bool D3, bool RAW>
+__global__ void __launch_bounds__(kThreads) kg_to_full(Grid g, const double* __restrict__ x, T* E, long npf,
+                                                       double czxy, double cyzx, double cxyz) {
+  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < g.n; n += gridDim.x * blockDim.x) {
+    int i, j, k;
+    node_ijk(g, n, i, j, k);
+    double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int c = 0; c < (D3 ? 5 : 4); ++c) v[c] = x[(long)c * g.npad + n];
+    write_eff<T, D3, RAW>(g, E, npf, i, j, k, v, czxy, cyzx, cxyz);
+  }
+}
+
+// Interior entries of a full-grid vector in T into a device-layout FP64 vector
+// (padding entries written as zero).
+template <typename T>
+__global__ void __launch_bounds__(kThreads) kg_from_full(Grid g, const T* __restrict__ E, long npf, double* x) {
+  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < g.npad; n += gridDim.x * blockDim.x) {
+    long m = 0;
+    if (n < g.n) {
+      int i, j, k;
+      node_ijk(g, n, i, j, k);
+      m = full_index(g, i, j, k);
+    }
+    for (int c = 0; c < g.ncomp; ++c) x[(long)c * g.npad + n] = n < g.n ? (double)E[(long)c * npf + m] : 0.0;
   }
 }
 

@@ -7,7 +7,10 @@
 
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include "tdgl_graph.cuh"
+#include "tdgl_tl.cuh"
 
 namespace tdgl {
 
@@ -22,6 +25,21 @@ struct Chain {
     p.blockDim = dim3(block);
     p.sharedMemBytes = (unsigned)smem;
     void* a[] = {&args};
+    p.kernelParams = a;
+    cudaGraphNode_t n;
+    cudaError_t e = cudaGraphAddKernelNode(&n, g, last ? &last : nullptr, last ? 1 : 0, &p);
+    if (e == cudaSuccess) last = n;
+    return e;
+  }
+  // kernel with a __grid_constant__ first parameter (the tensor maps) and the arguments
+  template <class M, class Args>
+  cudaError_t kernel2(const void* fn, dim3 grid, int block, size_t smem, const M& m, Args& args) {
+    cudaKernelNodeParams p{};
+    p.func = const_cast<void*>(fn);
+    p.gridDim = grid;
+    p.blockDim = dim3(block);
+    p.sharedMemBytes = (unsigned)smem;
+    void* a[] = {const_cast<M*>(&m), &args};
     p.kernelParams = a;
     cudaGraphNode_t n;
     cudaError_t e = cudaGraphAddKernelNode(&n, g, last ? &last : nullptr, last ? 1 : 0, &p);
@@ -50,8 +68,27 @@ struct Chain {
     if (e_ != cudaSuccess) return e_;    \
   } while (0)
 
+// Tangent-linear stencil node (Horner step when poly, else the Arnoldi
+// product): the TMA-staged kernel when tensor maps are given (FP32 vectors,
+// 3-D grids; `chunks` z-chunks), else the kernel that reads global memory.
 template <typename T, bool D3>
-cudaError_t build_trap_graph(GArgs<T> A, cudaGraph_t* out_graph, cudaGraphExec_t* out_exec) {
+cudaError_t add_tl(Chain& ch, const GArgs<T>& A, const TlMaps* tm, int chunks, bool poly) {
+  GArgs<T> a = A;
+  if constexpr (std::is_same<T, float>::value && D3) {
+    if (tm) {
+      const void* fn = poly ? (const void*)kg_tl<true> : (const void*)kg_tl<false>;
+      TDGL_GCK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTlSmem));
+      return ch.kernel2(fn, dim3(A.arn_gx, A.arn_gy, chunks), kThreads, kTlSmem, *tm, a);
+    }
+  }
+  const dim3 tiles(A.arn_gx, A.arn_gy, D3 ? A.g.nz : 1);
+  return ch.kernel(poly ? (const void*)kg_arn_poly<T, D3> : (const void*)kg_arn_apply<T, D3>, tiles, kThreads, 0,
+                   a);
+}
+
+template <typename T, bool D3>
+cudaError_t build_trap_graph(GArgs<T> A, const TlMaps* tm, int chunks, cudaGraph_t* out_graph,
+                             cudaGraphExec_t* out_exec) {
   cudaGraph_t G;
   TDGL_GCK(cudaGraphCreate(&G, 0));
   *out_graph = G;
@@ -83,7 +120,7 @@ cudaError_t build_trap_graph(GArgs<T> A, cudaGraph_t* out_graph, cudaGraphExec_t
       GArgs<T> P = A;
       P.pstep = k;
       P.pmode = 1;
-      TDGL_GCK(cn.kernel((const void*)kg_arn_poly<T, D3>, tiles, kThreads, 0, P));
+      TDGL_GCK((add_tl<T, D3>(cn, P, tm, chunks, true)));
     }
     GArgs<T> U = A;
     U.upd_single = 1;
@@ -107,7 +144,7 @@ cudaError_t build_trap_graph(GArgs<T> A, cudaGraph_t* out_graph, cudaGraphExec_t
       GArgs<T> P = A;
       P.pstep = k;
       P.pmode = 0;
-      TDGL_GCK(ck.kernel((const void*)kg_arn_poly<T, D3>, tiles, kThreads, 0, P));
+      TDGL_GCK((add_tl<T, D3>(ck, P, tm, chunks, true)));
     }
     if (A.apply_dots) {
       const size_t smp = apply_dots_smem<T>(A.kmax);
@@ -115,7 +152,7 @@ cudaError_t build_trap_graph(GArgs<T> A, cudaGraph_t* out_graph, cudaGraphExec_t
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smp));
       TDGL_GCK(ck.kernel((const void*)kg_arn_apply_dots<T, D3>, tiles, kThreads, smp, A));
     } else {
-      TDGL_GCK(ck.kernel((const void*)kg_arn_apply<T, D3>, tiles, kThreads, 0, A));
+      TDGL_GCK((add_tl<T, D3>(ck, A, tm, chunks, false)));
       TDGL_GCK(ck.kernel((const void*)kg_arn_dots<T>, A.nblk_arn, kThreads, smd, A));
     }
   } else {

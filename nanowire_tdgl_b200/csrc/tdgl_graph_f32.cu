@@ -4,16 +4,47 @@
 
 namespace tdgl {
 
-cudaError_t graph_build_f32(const GArgs<float>& A, cudaGraph_t* graph, cudaGraphExec_t* exec) {
-  if (A.g.is3d) return build_trap_graph<float, true>(A, graph, exec);
-  return build_trap_graph<float, false>(A, graph, exec);
+cudaError_t graph_build_f32(const GArgs<float>& A, const TlMaps* tm, int chunks, cudaGraph_t* graph,
+                            cudaGraphExec_t* exec) {
+  if (A.g.is3d) return build_trap_graph<float, true>(A, tm, chunks, graph, exec);
+  return build_trap_graph<float, false>(A, nullptr, 0, graph, exec);
+}
+
+// One tangent-linear stencil launch outside the graph (Horner step when poly,
+// else the product): the TMA-staged kernel when tm is given, else the kernel
+// that reads global memory.
+static cudaError_t launch_tl(const GArgs<float>& A, const TlMaps* tm, int chunks, bool poly, cudaStream_t s) {
+  if (A.g.is3d && tm) {
+    const void* fn = poly ? (const void*)kg_tl<true> : (const void*)kg_tl<false>;
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTlSmem);
+    if (e != cudaSuccess) return e;
+    const dim3 grid(A.arn_gx, A.arn_gy, chunks);
+    if (poly) kg_tl<true><<<grid, kThreads, kTlSmem, s>>>(*tm, A);
+    else kg_tl<false><<<grid, kThreads, kTlSmem, s>>>(*tm, A);
+    return cudaGetLastError();
+  }
+  const dim3 grid(A.arn_gx, A.arn_gy, A.g.is3d ? A.g.nz : 1);
+  if (poly) {
+    if (A.g.is3d) kg_arn_poly<float, true><<<grid, kThreads, 0, s>>>(A);
+    else kg_arn_poly<float, false><<<grid, kThreads, 0, s>>>(A);
+  } else {
+    if (A.g.is3d) kg_arn_apply<float, true><<<grid, kThreads, 0, s>>>(A);
+    else kg_arn_apply<float, false><<<grid, kThreads, 0, s>>>(A);
+  }
+  return cudaGetLastError();
+}
+
+// The Arnoldi product alone (the standalone Krylov-precision Jacobian product).
+cudaError_t product_f32(const GArgs<float>& A, const TlMaps* tm, int chunks, cudaStream_t s) {
+  return launch_tl(A, tm, chunks, false, s);
 }
 
 // Diagnostic: `launches` standalone Arnoldi steps.  kernels: bit 0 the
 // orthogonalisation, bit 1 the product, bit 2 the projections, bit 3 the fused
 // product and projections, bit 4 the polynomial preconditioner's steps (its
 // degree, before the product); 0 = the kernels of this context's graph.
-cudaError_t arnoldi_probe_f32(const GArgs<float>& A, int launches, int kernels, cudaStream_t s) {
+cudaError_t arnoldi_probe_f32(const GArgs<float>& A, const TlMaps* tm, int chunks, int launches, int kernels,
+                              cudaStream_t s) {
   const size_t smo = (size_t)(A.kmax + 1) * sizeof(double);
   const size_t smd = (size_t)kWarps * (A.kmax + 2) * sizeof(double);
   const size_t smp = apply_dots_smem<float>(A.kmax);
@@ -31,17 +62,14 @@ cudaError_t arnoldi_probe_f32(const GArgs<float>& A, int launches, int kernels, 
   const dim3 grid(A.arn_gx, A.arn_gy, A.g.is3d ? A.g.nz : 1);
   for (int r = 0; r < launches && e == cudaSuccess; ++r) {
     if (kernels & 1) kg_arn_orth<float><<<A.nblk_orth, kThreads, smo, s>>>(A);
-    for (int k = (kernels & 16) ? A.poly_deg - 1 : -1; k >= 0; --k) {
+    for (int k = (kernels & 16) ? A.poly_deg - 1 : -1; k >= 0 && e == cudaSuccess; --k) {
       GArgs<float> P = A;
       P.pstep = k;
       P.pmode = 0;
-      if (A.g.is3d) kg_arn_poly<float, true><<<grid, kThreads, 0, s>>>(P);
-      else kg_arn_poly<float, false><<<grid, kThreads, 0, s>>>(P);
+      e = launch_tl(P, tm, chunks, true, s);
     }
-    if (kernels & 2) {
-      if (A.g.is3d) kg_arn_apply<float, true><<<grid, kThreads, 0, s>>>(A);
-      else kg_arn_apply<float, false><<<grid, kThreads, 0, s>>>(A);
-    }
+    if ((kernels & 2) && e == cudaSuccess) e = launch_tl(A, tm, chunks, false, s);
+    if (e != cudaSuccess) break;
     if (kernels & 4) kg_arn_dots<float><<<A.nblk_arn, kThreads, smd, s>>>(A);
     if (kernels & 8) {
       if (A.g.is3d) kg_arn_apply_dots<float, true><<<grid, kThreads, smp, s>>>(A);

@@ -5,8 +5,16 @@
 namespace tdgl {
 
 cudaError_t graph_build_f64(const GArgs<double>& A, cudaGraph_t* graph, cudaGraphExec_t* exec) {
-  if (A.g.is3d) return build_trap_graph<double, true>(A, graph, exec);
-  return build_trap_graph<double, false>(A, graph, exec);
+  if (A.g.is3d) return build_trap_graph<double, true>(A, nullptr, 0, graph, exec);
+  return build_trap_graph<double, false>(A, nullptr, 0, graph, exec);
+}
+
+// The Arnoldi product alone (the standalone Krylov-precision Jacobian product).
+cudaError_t product_f64(const GArgs<double>& A, cudaStream_t s) {
+  const dim3 grid(A.arn_gx, A.arn_gy, A.g.is3d ? A.g.nz : 1);
+  if (A.g.is3d) kg_arn_apply<double, true><<<grid, kThreads, 0, s>>>(A);
+  else kg_arn_apply<double, false><<<grid, kThreads, 0, s>>>(A);
+  return cudaGetLastError();
 }
 
 // Diagnostic: `launches` standalone Arnoldi steps.  kernels: bit 0 the

@@ -141,8 +141,12 @@ class DeviceGrid:
 
     def jvp(self, x: torch.Tensor, p: torch.Tensor, dt: float, mode: str = "analytic", eps_mf: float = 1e-4,
             B=(0.0, 0.0, 0.0)) -> torch.Tensor:
+        """ap = p - dt/2 J(x) p.  mode "fd" / "analytic" (FP64), or "krylov": the
+        product as this context's analytic-product Krylov solves compute it
+        (FP32 for a mixed-precision context; the step graph's stencil kernel)."""
         out = self.empty_state()
-        L.check(self.lib.tdgl_jvp(self.handle, _ptr(x), _ptr(p), _ptr(out), float(dt), JVP_MODES[mode],
+        mid = L.TDGL_JVP_KRYLOV if mode == "krylov" else JVP_MODES[mode]
+        L.check(self.lib.tdgl_jvp(self.handle, _ptr(x), _ptr(p), _ptr(out), float(dt), mid,
                                   float(eps_mf), *map(float, B), stream_handle()), "tdgl_jvp")
         return out
 
@@ -257,6 +261,11 @@ class DeviceGrid:
         """Degree of the polynomial preconditioner of the analytic-product GMRES
         solves (0 off, -1 the default)."""
         L.check(self.lib.tdgl_ctx_set_poly(self.handle, int(degree)), "tdgl_ctx_set_poly")
+
+    def set_limits(self, wait_ns: int = 0, loop_cap: int = 0) -> None:
+        """Limits of the device's bounded waits (ns) and of one step-graph
+        launch's loop iterations; 0 restores the default."""
+        L.check(self.lib.tdgl_ctx_set_limits(self.handle, int(wait_ns), int(loop_cap)), "tdgl_ctx_set_limits")
 
     @property
     def poly_degree(self) -> int:

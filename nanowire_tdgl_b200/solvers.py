@@ -25,7 +25,12 @@ callable for every function value.
 Keyword-only additions: ``precision`` ("fp64" | "mixed"), ``jvp`` ("fd" |
 "analytic"), ``krylov`` ("gmres" | "gcr": the same minimal-residual iterates,
 GMRES storing one vector per iteration instead of GCR's two) and ``kmax``
-(Krylov directions held on the device).
+(Krylov directions held on the device).  The default Krylov method follows
+the product: with the reference's finite-difference product (the FP64
+default) it is the reference's own GCR (src/tdgl3d/solvers/tgcr.py:96-156),
+so a script switched over to this package gets the reference's method
+unless it asks for another; with analytic products (the mixed-precision
+default) it is GMRES with the polynomial preconditioner, the fast path.
 """
 
 from __future__ import annotations
@@ -51,6 +56,14 @@ from .model import (AppliedField, BoundaryVectors, StateVector, build_boundary_f
 DEFAULT_KMAX = 64
 
 
+def default_krylov(krylov: Optional[str], jvp: str) -> str:
+    """The Krylov method of a call: as given, else GCR (the reference's) for
+    finite-difference products and GMRES for analytic ones."""
+    if krylov is not None:
+        return krylov
+    return "gcr" if jvp == "fd" else "gmres"
+
+
 def _is_torch(x) -> bool:
     return isinstance(x, torch.Tensor)
 
@@ -68,12 +81,12 @@ class DeviceRHS:
     keeps the whole solve on the device."""
 
     def __init__(self, params, idx, B, material=None, precision: str = "fp64", jvp: Optional[str] = None,
-                 kmax: int = DEFAULT_KMAX, krylov: str = "gmres"):
+                 kmax: int = DEFAULT_KMAX, krylov: Optional[str] = None):
         self.params, self.idx, self.material = params, idx, material
         self.B = tuple(float(b) for b in B)
         self.precision = precision
         self.jvp = jvp or ("fd" if precision == "fp64" else "analytic")
-        self.grid = grid_for(params, idx, material, precision, kmax, krylov)
+        self.grid = grid_for(params, idx, material, precision, kmax, default_krylov(krylov, self.jvp))
 
     def __call__(self, X):
         return _out(self.grid.eval_f_ref(X, self.B), X)
@@ -358,7 +371,7 @@ def trapezoidal(x0, params, idx, eval_u: Callable, t_start: float, t_stop: float
                 tol_gcr: float = 1e-4, eps_mf: float = 1e-4, save_every: int = 1, adaptive: bool = True,
                 dt_min: float = 1e-8, progress: bool = True, verbose: bool = False, material=None,
                 precision: str = "fp64", jvp: Optional[str] = None, kmax: int = DEFAULT_KMAX,
-                krylov: str = "gmres", stats: Optional[dict] = None):
+                krylov: Optional[str] = None, stats: Optional[dict] = None):
     """Implicit trapezoidal integration with Newton-GCR and dt/10 retries
     (integrators.py:92-206).  Returns (times, X_history) with X_history of
     shape (n_state, n_saved), as the reference does.
@@ -369,7 +382,7 @@ def trapezoidal(x0, params, idx, eval_u: Callable, t_start: float, t_stop: float
     per step is made with the field evaluated on the host at the step's start.
     """
     jvp = jvp or ("fd" if precision == "fp64" else "analytic")
-    g = grid_for(params, idx, material, precision, kmax, krylov)
+    g = grid_for(params, idx, material, precision, kmax, default_krylov(krylov, jvp))
     _check_real_links(x0, params)
     x = g.pack(x0)
     opts = L.TrapOpts(float(t_stop), float(dt), float(dt_min), float(newton_tol_f), float(newton_tol_dx),
@@ -451,7 +464,7 @@ def solve(device, t_start: float = 0.0, t_stop: float = 10.0, dt: float = 0.05, 
           newton_tol_f: float = 1e-3, newton_tol_dx: float = 1e-3, newton_max_iter: int = 20,
           tol_gcr: float = 1e-4, eps_mf: float = 1e-4, adaptive: bool = True, log_metadata: bool = True,
           log_dir="logs", precision: str = "fp64", jvp: Optional[str] = None, kmax: int = DEFAULT_KMAX,
-          krylov: str = "gmres"):
+          krylov: Optional[str] = None):
     """Run a simulation and return a :class:`~nanowire_tdgl_b200.solution.Solution`
     (runner.py:40-163)."""
     from .solution import Solution
@@ -487,7 +500,9 @@ def solve(device, t_start: float = 0.0, t_stop: float = 10.0, dt: float = 0.05, 
                 "total_steps": int(len(times)), "params": {k: getattr(params, k) for k in
                 ("Nx", "Ny", "Nz", "hx", "hy", "hz", "kappa", "periodic_x", "periodic_y", "periodic_z")},
                 "newton_tol_f": newton_tol_f, "newton_tol_dx": newton_tol_dx, "tol_gcr": tol_gcr,
-                "precision": precision, "krylov": krylov, "device_counters": run_stats,
+                "precision": precision,
+                "krylov": default_krylov(krylov, jvp or ("fd" if precision == "fp64" else "analytic")),
+                "device_counters": run_stats,
                 "gpu": torch.cuda.get_device_name() if torch.cuda.is_available() else None}
         path = Path(log_dir)
         path.mkdir(parents=True, exist_ok=True)
