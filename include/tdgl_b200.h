@@ -228,9 +228,10 @@ int tdgl_adjoint_solve(tdgl_ctx* ctx, const double* x_dev, const double* b_dev, 
 /* tdgl_trap_run in two halves, for stepping many contexts concurrently (the
  * batched form; no reference counterpart): tdgl_trap_launch enqueues the
  * steps on the stream and returns at once (GMRES contexts only; x must stay
- * valid until the stream has passed them); after the stream has completed,
- * tdgl_trap_collect returns the clock, step size, counters and status.  One
- * uncollected launch per context at a time; while it is pending, the
+ * valid until the stream has passed them); tdgl_trap_collect waits for the
+ * launch and returns the clock, step size, counters and status.  One
+ * tdgl_trap_launch per context at a time (plus one tdgl_trap_launch_next
+ * queued behind it); while a launch is pending, the
  * context's other stepping entry points (tdgl_trap_run, tdgl_newton_trap,
  * tdgl_tgcr_trap, tdgl_euler_run, tdgl_arnoldi_probe, tdgl_ctx_set_blocks,
  * tdgl_ctx_set_poly)
@@ -238,6 +239,17 @@ int tdgl_adjoint_solve(tdgl_ctx* ctx, const double* x_dev, const double* b_dev, 
 int tdgl_trap_launch(tdgl_ctx* ctx, double* x_dev, double t, double dt_cur, int32_t max_steps,
                      const tdgl_trap_opts* opts, const tdgl_field* field, tdgl_stream_t stream);
 int tdgl_trap_collect(tdgl_ctx* ctx, double* t, double* dt_cur, tdgl_stats* stats);
+/* A continuation of the context's last step-graph launch (no reference
+ * counterpart; it keeps the loop of trapezoidal, integrators.py:150-197, on
+ * the device across calls): enqueues up to max_steps more steps on the
+ * stream, starting from the clock (t, dt_cur) and the state that the
+ * previous launch leaves, so that a caller can queue the next steps before it
+ * collects the previous ones (at most two launches queued per context).
+ * Launches are collected in order with tdgl_trap_collect, which waits for
+ * the launch it collects; a continuation whose clock has reached t_stop runs
+ * no step (steps = 0). */
+int tdgl_trap_launch_next(tdgl_ctx* ctx, double* x_dev, int32_t max_steps, const tdgl_trap_opts* opts,
+                          const tdgl_field* field, tdgl_stream_t stream);
 /* Launch shape of the step graph's grid kernels: block counts, each in
  * [1, 8 x SMs], of the grid-stride passes and of the Arnoldi streams (defaults
  * 8 and 5 blocks per SM), and whether the Arnoldi product and projections run

@@ -89,6 +89,7 @@ SIGNATURES = {
     "tdgl_ctx_set_blocks": (C.c_int, [_P, _I, _I, _I]),
     "tdgl_ctx_set_poly": (C.c_int, [_P, _I]),
     "tdgl_ctx_set_limits": (C.c_int, [_P, C.c_int64, C.c_int64]),
+    "tdgl_trap_launch_next": (C.c_int, [_P, _P, _I, C.POINTER(TrapOpts), C.POINTER(Field), _P]),
     "tdgl_ctx_poly_degree": (C.c_int32, [_P]),
     "tdgl_euler_run": (C.c_int, [_P, _P, C.POINTER(_D), _D, _D, _I, C.POINTER(Field), _P]),
     "tdgl_vjp": (C.c_int, [_P, _P, _P, _D, _D, _D, _P, _P, _P, _P, _P]),

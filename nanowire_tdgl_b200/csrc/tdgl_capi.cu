@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstddef>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -146,7 +147,16 @@ struct tdgl_ctx {
   double k2max = 0.0;
   void* PW[2] = {nullptr, nullptr};
   void* PC = nullptr;
-  bool pending = false, pending_noop = false;   // an uncollected tdgl_trap_launch
+  // queued step-graph launches (tdgl_trap_launch / tdgl_trap_launch_next):
+  // per launch slot a pinned input and output control block and a completion
+  // event; up to two launches queued, collected in order
+  GDev* gin[2] = {nullptr, nullptr};
+  GDev* gout[2] = {nullptr, nullptr};
+  cudaEvent_t gev[2] = {nullptr, nullptr};
+  double* gclk = nullptr;         // device: the clock (t, dt_cur) carried into a continuation
+  int npend = 0, pend_head = 0, next_slot = 0;
+  bool pend_noop[2] = {false, false};
+  bool has_clock = false;         // a launch has left its clock in the device control block
   uint8_t* imask = nullptr;
   uint32_t* deadmask = nullptr;   // per interior node: dead links read by the Arnoldi product
   uint8_t* ldead = nullptr;       // per full-grid node: its dead links (TMA-staged stencil)
@@ -288,6 +298,11 @@ extern "C" int tdgl_ctx_destroy(tdgl_ctx* c) {
   for (void* p : c->owned) cudaFree(p);
   if (c->ctl_host) cudaFreeHost(c->ctl_host);
   if (c->gdev_host) cudaFreeHost(c->gdev_host);
+  if (c->gin[1]) cudaFreeHost(c->gin[1]);
+  for (int k = 0; k < 2; ++k) {
+    if (c->gout[k]) cudaFreeHost(c->gout[k]);
+    if (c->gev[k]) cudaEventDestroy(c->gev[k]);
+  }
   delete c;
   return TDGL_OK;
 }
@@ -606,7 +621,7 @@ extern "C" int tdgl_tgcr_trap(tdgl_ctx* c, const double* x_lin, const double* bv
                               double tol, int32_t max_iter, double eps_mf, int32_t jvp_mode, double Bx, double By,
                               double Bz, tdgl_stats* st, tdgl_stream_t s) {
   if (!c || !x_lin || !bvec || !dvec) return fail(TDGL_EINVAL, "null argument");
-  if (c->pending) return fail(TDGL_EINVAL, "a launch of this context has not been collected");
+  if (c->npend) return fail(TDGL_EINVAL, "a launch of this context has not been collected");
   if (jvp_mode == TDGL_JVP_FD && c->precision == TDGL_MIXED)
     return fail(TDGL_EINVAL, "the finite-difference product needs the FP64 context");
   int rc;
@@ -633,7 +648,7 @@ extern "C" int tdgl_newton_trap(tdgl_ctx* c, double* x, const double* gamma, dou
                                 double tol_dx, int32_t max_iter, double tol_gcr, double eps_mf, int32_t jvp_mode,
                                 double Bx, double By, double Bz, tdgl_stats* st, tdgl_stream_t s) {
   if (!c || !x || !gamma) return fail(TDGL_EINVAL, "null argument");
-  if (c->pending) return fail(TDGL_EINVAL, "a launch of this context has not been collected");
+  if (c->npend) return fail(TDGL_EINVAL, "a launch of this context has not been collected");
   if (jvp_mode == TDGL_JVP_FD && c->precision == TDGL_MIXED)
     return fail(TDGL_EINVAL, "the finite-difference product needs the FP64 context");
   int rc;
@@ -791,8 +806,9 @@ static int apply_dots_setting(const tdgl_ctx* c) {
 // Tensor maps of the TMA-staged stencil over the context's FP32 full-grid
 // vectors (3-D grids; TDGL_TMA=0 keeps the stencil that reads global memory):
 // dimensions (x, y, z, component[, vector]) with the padded row pitch, boxes
-// of 36 x 10 x 1 x 5 entries.  z-chunks per tile column: TDGL_TL_CHUNKS, else
-// as many as keep every block of the launch resident at once (3 per SM).
+// of (32 NX + 4) x 10 x 1 x 5 entries for the kernel with NX nodes per thread
+// (TDGL_TL_NX, default 2).  z-chunks per tile column: TDGL_TL_CHUNKS, else as
+// many as keep every block of the launch resident at once.
 static int setup_tl(tdgl_ctx* c) {
   c->tl_on = false;
   const Grid& g = c->g;
@@ -813,7 +829,12 @@ static int setup_tl(tdgl_ctx* c) {
                               (cuuint64_t)c->kmax + 1};
   const cuuint64_t strides[4] = {(cuuint64_t)g.mj * fs, (cuuint64_t)g.mk * fs, (cuuint64_t)c->npf * fs,
                                  (cuuint64_t)kTlComp * (cuuint64_t)c->npf * fs};
-  const cuuint32_t box[5] = {(cuuint32_t)kTlBoxX, (cuuint32_t)kTlBoxY, 1u, (cuuint32_t)kTlComp, 1u};
+  // nodes per thread along x: TDGL_TL_NX (1 or 2), else 2
+  int tnx = 2;
+  if (const char* e = std::getenv("TDGL_TL_NX"))
+    if (std::atoi(e) == 1 || std::atoi(e) == 2) tnx = std::atoi(e);
+  c->tlm.nx = tnx;
+  const cuuint32_t box[5] = {(cuuint32_t)(32 * tnx + 4), (cuuint32_t)kTlBoxY, 1u, (cuuint32_t)kTlComp, 1u};
   const cuuint32_t es[5] = {1u, 1u, 1u, 1u, 1u};
   if (g.ncomp != kTlComp || g.mj % 4 || c->npf % 4) return fail(TDGL_ECUDA, "full-grid layout not TMA-aligned");
   void* base[5] = {c->XLe, c->UB, c->PW[0], c->PW[1], c->PC};
@@ -824,8 +845,9 @@ static int setup_tl(tdgl_ctx* c) {
                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return fail(TDGL_ECUDA, "cuTensorMapEncodeTiled failed (code " + std::to_string((int)r) + ")");
   }
-  const int tiles = c->arn_gx * c->arn_gy;
-  int ch = std::max(1, (c->num_sms * 3) / std::max(tiles, 1));
+  const int tiles = tl_grid_x(g.nx, tnx) * c->arn_gy;
+  const int resident = tnx == 2 ? TlShape<2>::kMinBlocks : TlShape<1>::kMinBlocks;
+  int ch = std::max(1, (c->num_sms * resident) / std::max(tiles, 1));
   if (const char* e = std::getenv("TDGL_TL_CHUNKS"))
     if (std::atoi(e) > 0) ch = std::atoi(e);
   c->tl_chunks = std::min(std::max(ch, 1), g.nz);
@@ -923,6 +945,12 @@ static int ensure_graph(tdgl_ctx* c, int v) {
     if ((rc = ctx_alloc(c, (void**)&c->kry, sizeof(double) * kry_len(c->kmax)))) return rc;
     if ((rc = ctx_alloc(c, (void**)&c->gdev, sizeof(GDev)))) return rc;
     TDGL_CUDA(cudaMallocHost((void**)&c->gdev_host, sizeof(GDev)));
+    c->gin[0] = c->gdev_host;
+    TDGL_CUDA(cudaMallocHost((void**)&c->gin[1], sizeof(GDev)));
+    TDGL_CUDA(cudaMallocHost((void**)&c->gout[0], sizeof(GDev)));
+    TDGL_CUDA(cudaMallocHost((void**)&c->gout[1], sizeof(GDev)));
+    for (int k = 0; k < 2; ++k) TDGL_CUDA(cudaEventCreateWithFlags(&c->gev[k], cudaEventDisableTiming));
+    if ((rc = ctx_alloc(c, (void**)&c->gclk, 2 * sizeof(double)))) return rc;
     const char* pe = std::getenv("TDGL_PROFILE");
     c->gprof = pe && pe[0] && pe[0] != '0';
     c->gws_ready = true;
@@ -952,6 +980,7 @@ static int ensure_graph(tdgl_ctx* c, int v) {
 static int graph_status(int gs) {
   switch (gs) {
     case GS_OK: return TDGL_OK;
+    case GS_IDLE: return TDGL_OK;
     case GS_NOCONV: return TDGL_ENOCONV;
     case GS_DTMIN: return TDGL_EDTMIN;
     case GS_KMAX: return TDGL_EKMAX;
@@ -961,13 +990,17 @@ static int graph_status(int gs) {
 }
 
 // Enqueue one graph launch for up to max_steps steps on stream s (no
-// synchronisation); *noop is set when nothing needs to run.
+// synchronisation) with the control blocks of launch slot `slot`; *noop is
+// set when nothing needs to run.  cont: a continuation, which starts from the
+// clock (t, dt_cur) the previous launch left in the device control block
+// instead of (t0, cur0); the device's own step loop test decides whether it
+// runs any step.  The slot's event is recorded after the launch's outputs.
 static int graph_launch(tdgl_ctx* c, double* x, double t0, double cur0, int32_t max_steps, const tdgl_trap_opts* o,
-                        const tdgl_field* f, tdgl_stream_t s, bool* noop) {
+                        const tdgl_field* f, tdgl_stream_t s, bool* noop, int slot = 0, bool cont = false) {
   int rc;
   const int v = o->jvp_mode == TDGL_JVP_ANALYTIC ? 1 : 0;
   if ((rc = ensure_graph(c, v))) return rc;
-  GDev& h = *c->gdev_host;
+  GDev& h = *c->gin[slot];
   std::memset(&h, 0, sizeof(GDev));
   h.t = t0;
   h.dt_cur = cur0;
@@ -996,21 +1029,28 @@ static int graph_launch(tdgl_ctx* c, double* x, double t0, double cur0, int32_t 
   h.wait_ns = c->wait_ns;
   h.prof_on = c->gprof ? 1 : 0;
   for (int k = 0; k < kKTypes; ++k) h.kt_start[k] = ~0ull;
-  *noop = !(h.t < h.t_stop - 1e-14) || max_steps <= 0;
+  *noop = max_steps <= 0 || (!cont && !(h.t < h.t_stop - 1e-14));
   if (*noop) return TDGL_OK;
+  static_assert(offsetof(GDev, dt_cur) == offsetof(GDev, t) + sizeof(double), "clock layout");
+  char* clk = (char*)c->gdev + offsetof(GDev, t);
   TDGL_CUDA(cudaMemcpyAsync(c->Xn, x, c->L * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  if (cont) TDGL_CUDA(cudaMemcpyAsync(c->gclk, clk, 2 * sizeof(double), cudaMemcpyDeviceToDevice, s));
   TDGL_CUDA(cudaMemcpyAsync(c->gdev, &h, sizeof(GDev), cudaMemcpyHostToDevice, s));
+  if (cont) TDGL_CUDA(cudaMemcpyAsync(clk, c->gclk, 2 * sizeof(double), cudaMemcpyDeviceToDevice, s));
   if (c->ticket) TDGL_CUDA(cudaMemsetAsync(c->ticket, 0, sizeof(unsigned), s));
   if (c->gticket) TDGL_CUDA(cudaMemsetAsync(c->gticket, 0, sizeof(unsigned) * (size_t)c->ngroups_cap, s));
   TDGL_CUDA(cudaGraphLaunch(c->gexec[v], s));
-  TDGL_CUDA(cudaMemcpyAsync(&h, c->gdev, sizeof(GDev), cudaMemcpyDeviceToHost, s));
+  TDGL_CUDA(cudaMemcpyAsync(c->gout[slot], c->gdev, sizeof(GDev), cudaMemcpyDeviceToHost, s));
   TDGL_CUDA(cudaMemcpyAsync(x, c->Xn, c->L * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  TDGL_CUDA(cudaEventRecord(c->gev[slot], s));
+  c->has_clock = true;
   return TDGL_OK;
 }
 
-// Results of the last graph_launch once its stream has completed.
-static int graph_collect(tdgl_ctx* c, bool noop, double* t, double* dt_cur, tdgl_stats* st) {
-  GDev& h = *c->gdev_host;
+// Results of the graph_launch of slot `slot` (waits for its event).
+static int graph_collect(tdgl_ctx* c, bool noop, double* t, double* dt_cur, tdgl_stats* st, int slot = 0) {
+  if (!noop) TDGL_CUDA(cudaEventSynchronize(c->gev[slot]));
+  GDev& h = noop ? *c->gin[slot] : *c->gout[slot];
   if (tdgl_stats* z = st) std::memset(z, 0, sizeof(*z));
   *t = h.t;
   *dt_cur = h.dt_cur;
@@ -1056,7 +1096,7 @@ static int run_graph(tdgl_ctx* c, double* x, double* t, double* dt_cur, int32_t 
 extern "C" int tdgl_adjoint_solve(tdgl_ctx* c, const double* x, const double* b, double* mu, double h, double tol,
                                   double Bx, double By, double Bz, int32_t* iters, tdgl_stream_t s) {
   if (!c || !x || !b || !mu) return fail(TDGL_EINVAL, "null argument");
-  if (c->pending) return fail(TDGL_EINVAL, "a launch of this context has not been collected");
+  if (c->npend) return fail(TDGL_EINVAL, "a launch of this context has not been collected");
   if (c->precision != TDGL_FP64) return fail(TDGL_EINVAL, "the adjoint solve needs an FP64 context");
   int rc;
   if ((rc = ensure_graph(c, 0))) return rc;            // the stepper workspace the solve shares
@@ -1080,6 +1120,7 @@ extern "C" int tdgl_adjoint_solve(tdgl_ctx* c, const double* x, const double* b,
       return fail(TDGL_ECUDA, std::string("building the adjoint graph: ") + cudaGetErrorString(e));
     }
   }
+  c->has_clock = false;                          // the device control block is reused below
   GDev& hd = *c->gdev_host;
   std::memset(&hd, 0, sizeof(GDev));
   hd.dta = 2.0 * h;
@@ -1106,17 +1147,42 @@ extern "C" int tdgl_trap_launch(tdgl_ctx* c, double* x, double t, double dt_cur,
   if (o->jvp_mode == TDGL_JVP_FD && c->precision == TDGL_MIXED)
     return fail(TDGL_EINVAL, "the finite-difference product needs the FP64 context");
   if (c->krylov != KRY_GMRES) return fail(TDGL_EINVAL, "asynchronous stepping needs the GMRES graph executor");
-  if (c->pending) return fail(TDGL_EINVAL, "a launch of this context has not been collected");
-  int rc = graph_launch(c, x, t, dt_cur, max_steps, o, f, s, &c->pending_noop);
-  if (rc == TDGL_OK) c->pending = true;
+  if (c->npend) return fail(TDGL_EINVAL, "a launch of this context has not been collected");
+  const int slot = c->next_slot;
+  int rc = graph_launch(c, x, t, dt_cur, max_steps, o, f, s, &c->pend_noop[slot], slot, false);
+  if (rc == TDGL_OK) {
+    c->pend_head = slot;
+    c->npend = 1;
+    c->next_slot = slot ^ 1;
+  }
+  return rc;
+}
+
+extern "C" int tdgl_trap_launch_next(tdgl_ctx* c, double* x, int32_t max_steps, const tdgl_trap_opts* o,
+                                     const tdgl_field* f, tdgl_stream_t s) {
+  if (!c || !x || !o || !f) return fail(TDGL_EINVAL, "null argument");
+  if (o->jvp_mode == TDGL_JVP_FD && c->precision == TDGL_MIXED)
+    return fail(TDGL_EINVAL, "the finite-difference product needs the FP64 context");
+  if (c->krylov != KRY_GMRES) return fail(TDGL_EINVAL, "asynchronous stepping needs the GMRES graph executor");
+  if (c->npend > 1) return fail(TDGL_EINVAL, "two launches of this context are already queued");
+  if (!c->has_clock) return fail(TDGL_EINVAL, "no earlier launch of this context to continue");
+  const int slot = c->next_slot;
+  int rc = graph_launch(c, x, 0.0, 0.0, max_steps, o, f, s, &c->pend_noop[slot], slot, true);
+  if (rc == TDGL_OK) {
+    if (c->npend == 0) c->pend_head = slot;
+    ++c->npend;
+    c->next_slot = slot ^ 1;
+  }
   return rc;
 }
 
 extern "C" int tdgl_trap_collect(tdgl_ctx* c, double* t, double* dt_cur, tdgl_stats* st) {
   if (!c || !t || !dt_cur) return fail(TDGL_EINVAL, "null argument");
-  if (!c->pending) return fail(TDGL_EINVAL, "no launch to collect");
-  c->pending = false;
-  return graph_collect(c, c->pending_noop, t, dt_cur, st);
+  if (!c->npend) return fail(TDGL_EINVAL, "no launch to collect");
+  const int slot = c->pend_head;
+  c->pend_head ^= 1;
+  --c->npend;
+  return graph_collect(c, c->pend_noop[slot], t, dt_cur, st, slot);
 }
 
 extern "C" int tdgl_ctx_set_blocks(tdgl_ctx* c, int32_t stream_blocks, int32_t krylov_blocks, int32_t fused) {
@@ -1124,7 +1190,7 @@ extern "C" int tdgl_ctx_set_blocks(tdgl_ctx* c, int32_t stream_blocks, int32_t k
   const int cap = c->num_sms * kMaxBlocksPerSm;
   if (stream_blocks < 1 || stream_blocks > cap || krylov_blocks < 1 || krylov_blocks > cap)
     return fail(TDGL_EINVAL, "block counts must lie in [1, 8 x SMs]");
-  if (c->pending) return fail(TDGL_EINVAL, "a launch of this context has not been collected");
+  if (c->npend) return fail(TDGL_EINVAL, "a launch of this context has not been collected");
   c->blk_stream = stream_blocks;
   c->blk_krylov = krylov_blocks;
   c->apply_dots_req = fused < 0 ? -1 : (fused ? 1 : 0);
@@ -1142,7 +1208,7 @@ extern "C" int tdgl_ctx_set_blocks(tdgl_ctx* c, int32_t stream_blocks, int32_t k
 extern "C" int tdgl_ctx_set_poly(tdgl_ctx* c, int32_t degree) {
   if (!c) return fail(TDGL_EINVAL, "null argument");
   if (degree < -1 || degree > kPolyMax) return fail(TDGL_EINVAL, "polynomial degree must lie in [-1, 8]");
-  if (c->pending) return fail(TDGL_EINVAL, "a launch of this context has not been collected");
+  if (c->npend) return fail(TDGL_EINVAL, "a launch of this context has not been collected");
   c->poly_req = degree;
   if (c->UB) c->poly_deg = poly_setting(c);
   if (c->gexec[1]) cudaGraphExecDestroy(c->gexec[1]);   // the analytic-product graph is rebuilt at the next launch
@@ -1160,7 +1226,7 @@ extern "C" int32_t tdgl_ctx_poly_degree(const tdgl_ctx* c) {
 extern "C" int tdgl_trap_run(tdgl_ctx* c, double* x, double* t, double* dt_cur, int32_t max_steps,
                              const tdgl_trap_opts* o, const tdgl_field* f, tdgl_stats* st, tdgl_stream_t s) {
   if (!c || !x || !t || !dt_cur || !o || !f) return fail(TDGL_EINVAL, "null argument");
-  if (c->pending) return fail(TDGL_EINVAL, "a launch of this context has not been collected");
+  if (c->npend) return fail(TDGL_EINVAL, "a launch of this context has not been collected");
   if (o->jvp_mode == TDGL_JVP_FD && c->precision == TDGL_MIXED)
     return fail(TDGL_EINVAL, "the finite-difference product needs the FP64 context");
   if (c->krylov == KRY_GMRES) return run_graph(c, x, t, dt_cur, max_steps, o, f, st, s);
@@ -1215,7 +1281,7 @@ static void host_field(const tdgl_field* f, double t, double& bx, double& by, do
 extern "C" int tdgl_euler_run(tdgl_ctx* c, double* x, double* t, double t_stop, double dt, int32_t n_steps,
                               const tdgl_field* f, tdgl_stream_t s) {
   if (!c || !x || !t || !f) return fail(TDGL_EINVAL, "null argument");
-  if (c->pending) return fail(TDGL_EINVAL, "a launch of this context has not been collected");
+  if (c->npend) return fail(TDGL_EINVAL, "a launch of this context has not been collected");
   double* a = x;
   double* b = c->s_x;
   for (int i = 0; i < n_steps; ++i) {
@@ -1240,11 +1306,12 @@ extern "C" int tdgl_euler_run(tdgl_ctx* c, double* x, double* t, double t_stop, 
 // bounded wait that ran out.
 static int krylov_product(tdgl_ctx* c, const double* x, const double* p, double* ap, double dt, double Bx,
                           double By, double Bz, tdgl_stream_t s) {
-  if (c->pending) return fail(TDGL_EINVAL, "a launch of this context has not been collected");
+  if (c->npend) return fail(TDGL_EINVAL, "a launch of this context has not been collected");
   int rc;
   if ((rc = ensure_graph(c, 1))) return rc;
   const Grid& g = c->g;
   const BTerms<double> b = bterms(g, Bx, By, Bz);
+  c->has_clock = false;                          // the device control block is reused below
   GDev& h = *c->gdev_host;
   std::memset(&h, 0, sizeof(GDev));
   h.dta = dt;
@@ -1291,7 +1358,7 @@ static int krylov_product(tdgl_ctx* c, const double* x, const double* p, double*
 
 extern "C" int tdgl_ctx_set_limits(tdgl_ctx* c, int64_t wait_ns, int64_t loop_cap) {
   if (!c) return fail(TDGL_EINVAL, "null context");
-  if (c->pending) return fail(TDGL_EINVAL, "a launch of this context has not been collected");
+  if (c->npend) return fail(TDGL_EINVAL, "a launch of this context has not been collected");
   c->wait_ns = wait_ns > 0 ? (unsigned long long)wait_ns : kWaitDefaultNs;
   c->watchdog_req = loop_cap > 0 ? loop_cap : 0;
   return TDGL_OK;
@@ -1299,10 +1366,11 @@ extern "C" int tdgl_ctx_set_limits(tdgl_ctx* c, int64_t wait_ns, int64_t loop_ca
 
 extern "C" int tdgl_arnoldi_probe(tdgl_ctx* c, int32_t ja, int32_t launches, int32_t kernels, tdgl_stream_t s) {
   if (!c || launches < 0) return fail(TDGL_EINVAL, "invalid argument");
-  if (c->pending) return fail(TDGL_EINVAL, "a launch of this context has not been collected");
+  if (c->npend) return fail(TDGL_EINVAL, "a launch of this context has not been collected");
   int rc;
   if ((rc = ensure_graph(c, 1))) return rc;
   if (ja < 0 || ja > c->kmax) return fail(TDGL_EINVAL, "ja must lie in [0, kmax]");
+  c->has_clock = false;
   TDGL_CUDA(cudaMemcpyAsync(&c->gdev->ja, &ja, sizeof(int), cudaMemcpyHostToDevice, s));
   cudaError_t e;
   if (c->precision == TDGL_MIXED) {

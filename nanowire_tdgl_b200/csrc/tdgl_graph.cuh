@@ -36,8 +36,11 @@
 namespace tdgl {
 
 // GS_CAP: a loop ran past its watchdog count; GS_TIMEOUT: a bounded wait of a
-// kernel ran out (TMA-staged stencil).
-enum GStatus : int { GS_OK = 0, GS_NOCONV = 1, GS_DTMIN = 2, GS_KMAX = 3, GS_NONFINITE = 4, GS_CAP = 5, GS_TIMEOUT = 6 };
+// kernel ran out (TMA-staged stencil); GS_IDLE: the launch found its clock at
+// t_stop and made no step (a continuation launch; reported as success).
+enum GStatus : int {
+  GS_OK = 0, GS_NOCONV = 1, GS_DTMIN = 2, GS_KMAX = 3, GS_NONFINITE = 4, GS_CAP = 5, GS_TIMEOUT = 6, GS_IDLE = 7
+};
 
 constexpr int kKTypes = 16;   // slots of the per-kernel timers
 
@@ -1030,6 +1033,7 @@ __global__ void __launch_bounds__(kThreads, 3) kg_arn_apply(GArgs<T> A) {
       if (!nc.material) nc.sc = T(1);
       else if (nf & NF_SCFRAC) nc.sc = (T)g.scint[n];
       else nc.sc = (nf & NF_SC0) ? T(0) : T(1);
+      set_ih(g, nc);
     }
     NbEro<T> X{A.XLe, npf, m, g.mj, g.mk};
     NbMk<T> P{Uj, npf, m, g.mj, g.mk, A.deadmask[n], NbM<T>{Uj, npf, m, g.mj, g.mk, i, j, k, &g, g.lflags}};
@@ -1129,6 +1133,7 @@ __global__ void __launch_bounds__(kThreads, 3) kg_arn_poly(GArgs<T> A) {
       if (!nc.material) nc.sc = T(1);
       else if (nf & NF_SCFRAC) nc.sc = (T)g.scint[n];
       else nc.sc = (nf & NF_SC0) ? T(0) : T(1);
+      set_ih(g, nc);
     }
     NbEro<T> X{A.XLe, npf, m, g.mj, g.mk};
     NbMk<T> P{Win, npf, m, g.mj, g.mk, A.deadmask[n], NbM<T>{Win, npf, m, g.mj, g.mk, i, j, k, &g, g.lflags}};
@@ -1383,6 +1388,7 @@ __global__ void __launch_bounds__(kThreads, 3) kg_arn_apply_dots(GArgs<T> A) {
       if (!nc.material) nc.sc = T(1);
       else if (nf & NF_SCFRAC) nc.sc = (T)g.scint[n];
       else nc.sc = (nf & NF_SC0) ? T(0) : T(1);
+      set_ih(g, nc);
     }
     NbEro<T> X{A.XLe, npf, m, g.mj, g.mk};
     NbMk<T> P{Uj, npf, m, g.mj, g.mk, A.deadmask[n], NbM<T>{Uj, npf, m, g.mj, g.mk, i, j, k, &g, g.lflags}};
@@ -1462,6 +1468,9 @@ __global__ void kg_step_begin(GArgs<T> A) {
   if (threadIdx.x != 0) return;
   GDev* d = A.dev;
   if (d->status != GS_OK) return;
+  // the loop test of integrators.py:150 before the first step of a launch
+  // (a continuation launch takes its clock from the launch before it)
+  if (!(d->t < d->t_stop - 1e-14) || d->steps >= d->max_steps) { abort_all(A, GS_IDLE); return; }
   if (++d->watchdog > d->watchdog_cap) { abort_all(A, GS_CAP); return; }
   d->dta = fmin(d->dt_cur, d->t_stop - d->t);
   double bx, by, bz;

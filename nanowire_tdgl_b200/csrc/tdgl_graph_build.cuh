@@ -76,9 +76,11 @@ cudaError_t add_tl(Chain& ch, const GArgs<T>& A, const TlMaps* tm, int chunks, b
   GArgs<T> a = A;
   if constexpr (std::is_same<T, float>::value && D3) {
     if (tm) {
-      const void* fn = poly ? (const void*)kg_tl<true> : (const void*)kg_tl<false>;
-      TDGL_GCK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTlSmem));
-      return ch.kernel2(fn, dim3(A.arn_gx, A.arn_gy, chunks), kThreads, kTlSmem, *tm, a);
+      const void* fn = tm->nx == 2 ? (poly ? (const void*)kg_tl<true, 2> : (const void*)kg_tl<false, 2>)
+                                   : (poly ? (const void*)kg_tl<true, 1> : (const void*)kg_tl<false, 1>);
+      const size_t smem = tl_smem_bytes(tm->nx);
+      TDGL_GCK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      return ch.kernel2(fn, dim3(tl_grid_x(A.g.nx, tm->nx), A.arn_gy, chunks), kThreads, smem, *tm, a);
     }
   }
   const dim3 tiles(A.arn_gx, A.arn_gy, D3 ? A.g.nz : 1);

@@ -15,13 +15,14 @@ cudaError_t graph_build_f32(const GArgs<float>& A, const TlMaps* tm, int chunks,
 // that reads global memory.
 static cudaError_t launch_tl(const GArgs<float>& A, const TlMaps* tm, int chunks, bool poly, cudaStream_t s) {
   if (A.g.is3d && tm) {
-    const void* fn = poly ? (const void*)kg_tl<true> : (const void*)kg_tl<false>;
-    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTlSmem);
+    const void* fn = tm->nx == 2 ? (poly ? (const void*)kg_tl<true, 2> : (const void*)kg_tl<false, 2>)
+                                 : (poly ? (const void*)kg_tl<true, 1> : (const void*)kg_tl<false, 1>);
+    const size_t smem = tl_smem_bytes(tm->nx);
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    const dim3 grid(A.arn_gx, A.arn_gy, chunks);
-    if (poly) kg_tl<true><<<grid, kThreads, kTlSmem, s>>>(*tm, A);
-    else kg_tl<false><<<grid, kThreads, kTlSmem, s>>>(*tm, A);
-    return cudaGetLastError();
+    const dim3 grid(tl_grid_x(A.g.nx, tm->nx), A.arn_gy, chunks);
+    void* args[] = {const_cast<TlMaps*>(tm), const_cast<GArgs<float>*>(&A)};
+    return cudaLaunchKernel(fn, grid, dim3(kThreads), args, smem, s);
   }
   const dim3 grid(A.arn_gx, A.arn_gy, A.g.is3d ? A.g.nz : 1);
   if (poly) {

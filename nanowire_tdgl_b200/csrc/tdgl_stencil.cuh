@@ -230,7 +230,15 @@ struct NodeCoef {
   T cx, cy, cz;     // kappa(m)^2 / h^2 (cz = 0 in 2-D)
   T sc;             // superconducting fraction (1 without material)
   bool material;
+  T ihx, ihy, ihz;  // 1 / h^2 of the psi Laplacian
 };
+
+template <typename T>
+TDGL_HD void set_ih(const Grid& g, NodeCoef<T>& nc) {
+  nc.ihx = (T)g.ihx2;
+  nc.ihy = (T)g.ihy2;
+  nc.ihz = (T)g.ihz2;
+}
 
 template <typename T>
 TDGL_HD NodeCoef<T> node_coef(const Grid& g, int d, uint8_t nf) {
@@ -243,6 +251,7 @@ TDGL_HD NodeCoef<T> node_coef(const Grid& g, int d, uint8_t nf) {
   if (!nc.material) nc.sc = T(1);
   else if (nf & NF_SCFRAC) nc.sc = (T)g.scint[d];
   else nc.sc = (nf & NF_SC0) ? T(0) : T(1);
+  set_ih(g, nc);
   return nc;
 }
 
@@ -354,7 +363,7 @@ TDGL_HD void jvp_body(const Grid& g, const AXs& X, const APs& P, const NodeCoef<
     // d[e^{i a0} pp] = e^{i a0} (dpp + i da0 pp)
     T wr = qpr - da0 * ppi, wi = qpi + da0 * ppr;
     T lpr = c0 * wr - s0 * wi, lpi = c0 * wi + s0 * wr;
-    T ih = (T)(a == 0 ? g.ihx2 : (a == 1 ? g.ihy2 : g.ihz2));
+    const T ih = a == 0 ? nc.ihx : (a == 1 ? nc.ihy : nc.ihz);
     dre += (lmr - T(2) * dcr + lpr) * ih;
     dim += (lmi - T(2) * dci + lpi) * ih;
     // d Im[e^{-i a0} conj(psi) psi1]

@@ -7,18 +7,20 @@
 // Z = W - dt/2 J(x) W, or one Horner step of the polynomial preconditioner,
 // W_k = e_k V + beta ((W_in - dt/2 J W_in) - theta W_in) / delta.
 //
-// Each block owns a 32 x 8 tile of interior nodes (one per thread) and marches
-// through a range of z-planes.  For every plane it stages a 36 x 10 box of the
-// linearisation copy and of the direction vector (all components; the box
-// starts one node before the tile in x and y, so the tile's x- and y-neighbours
-// are in it) into a ring of five shared-memory slots with
-// cp.async.bulk.tensor, one elected thread issuing the copies, each slot
-// guarded by an mbarrier that the copies complete.  A node then reads its
-// 3 x 3 x 3 neighbourhood from the slots of planes k - 1, k and k + 1 with
-// constant offsets, and the direction's dead links (normal links on plane
-// N - 1 of their axis, hole links) are zeroed on the read from the node's
-// 27-bit mask; warps whose nodes read no dead link skip the selects.  Planes
-// k + 2 and k + 3 are in flight while plane k is computed.
+// Each block owns a (32 NX) x 8 tile of interior nodes (NX nodes per thread,
+// 32 apart in x; NX = 1 or 2) and marches through a range of z-planes.  For
+// every plane it stages a (32 NX + 4) x 10 box of the linearisation copy and
+// of the direction vector (all components; the box starts one node before
+// the tile in x and y, so the tile's x- and y-neighbours are in it) into a
+// ring of shared-memory slots with cp.async.bulk.tensor, one elected thread
+// issuing the copies, each slot guarded by an mbarrier that the copies
+// complete.  Once a plane has landed, the threads zero the direction's dead
+// links in it (normal links on plane N - 1 of their axis, hole links; each
+// thread its own positions and one position of the ring around the tile),
+// keeping their own raw values; a node then reads its 3 x 3 x 3
+// neighbourhood from the slots of planes k - 1, k and k + 1 with constant
+// offsets and no selects.  The planes after k + 1 are in flight while plane
+// k is computed.
 //
 // Layout requirements (met by the context): full-grid rows padded to a
 // multiple of 4 entries (16 bytes of FP32), component and vector strides
@@ -41,19 +43,26 @@
 
 namespace tdgl {
 
-constexpr int kTlTx = 32, kTlTy = 8;                  // tile: one node per thread
-constexpr int kTlBoxX = kTlTx + 4;                    // staged x extent: i0 - 1 .. i0 + 34 (144 bytes)
+constexpr int kTlTy = 8;                              // tile rows (threads per column of the block)
 constexpr int kTlBoxY = kTlTy + 2;                    // staged y extent: j0 - 1 .. j0 + 8
-constexpr int kTlPlane = kTlBoxX * kTlBoxY;           // entries per component and plane
 constexpr int kTlComp = 5;                            // components of a 3-D vector
-constexpr unsigned kTlBytes = kTlComp * kTlPlane * 4; // bytes of one staged box (7,200)
-constexpr int kTlSlotF = 1824;                        // floats per staged box, rounded up to 128 bytes
-constexpr int kTlSlots = 5;                           // ring of staged planes
-constexpr size_t kTlSmem = (size_t)kTlSlots * 2 * kTlSlotF * sizeof(float);   // 72,960 bytes
 constexpr unsigned long long kTlDrainNs = 2000000000ull;   // bound of the wait for copies in flight
-#ifndef TDGL_TL_MINB
-#define TDGL_TL_MINB 3                                // resident blocks per SM the register budget allows
-#endif
+
+// Shapes of the kernel with NX nodes per thread.
+template <int NX>
+struct TlShape {
+  static constexpr int kTx = 32 * NX;                        // tile width
+  static constexpr int kBoxX = kTx + 4;                      // staged x extent: i0 - 1 .. i0 + kTx + 2 (16-byte multiple)
+  static constexpr int kPlane = kBoxX * kTlBoxY;             // entries per component and plane
+  static constexpr unsigned kBytes = kTlComp * kPlane * 4;   // bytes of one staged box
+  static constexpr int kSlotF = (kTlComp * kPlane + 31) / 32 * 32;   // floats per box, rounded up to 128 bytes
+  static constexpr int kSlots = NX == 1 ? 5 : 4;             // ring of staged planes
+  static constexpr int kAhead = kSlots - 2;                  // planes issued ahead of the one being waited for
+  static constexpr size_t kSmem = (size_t)kSlots * 2 * kSlotF * sizeof(float);
+  static constexpr int kRing = 2 * (kTx + 2) + 2 * kTlTy;    // positions around the tile that are read
+  static constexpr int kMinBlocks = NX == 1 ? 3 : 2;         // resident blocks per SM (shared memory)
+  static_assert((kSlotF * 4) % 128 == 0 && kRing <= 256 && (kBoxX * 4) % 16 == 0, "staged box shape");
+};
 
 // Tensor maps of the staged vectors: 0 linearisation copy, 1 the basis (5-D:
 // the fifth coordinate is the basis vector), 2 and 3 the Horner buffers, 4 the
@@ -61,9 +70,13 @@ constexpr unsigned long long kTlDrainNs = 2000000000ull;   // bound of the wait 
 enum TlMap : int { TM_X = 0, TM_UB = 1, TM_PW0 = 2, TM_PW1 = 3, TM_PC = 4 };
 struct alignas(64) TlMaps {
   CUtensorMap m[5];
+  int nx;        // nodes per thread along x of the kernel the maps' boxes are shaped for (1 or 2)
 };
 
-static_assert(kTlSlotF >= kTlComp * kTlPlane && (kTlSlotF * 4) % 128 == 0, "staged box slot");
+// Launch shape of kg_tl<.., NX>: grid width and dynamic shared memory.
+__host__ __device__ inline int tl_grid_x(int nx, int NX) { return (nx + 32 * NX - 1) / (32 * NX); }
+inline size_t tl_smem_bytes(int NX);
+
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -118,27 +131,29 @@ __device__ __forceinline__ void tma_load5(float* dst, const CUtensorMap* m, int 
       : "memory");
 }
 
-// Dynamic shared memory of kg_tl: [kTlSlots][2][kTlSlotF] floats (per slot the
+// Dynamic shared memory of kg_tl: [slots][2][kSlotF] floats (per slot the
 // linearisation's box, then the direction's).
 extern __shared__ __align__(128) float tl_smem[];
 
 // Neighbourhood of a node in the staged boxes of planes k - 1, k, k + 1:
 // entry offsets (in floats) of the node's position in the three boxes; the
-// neighbour reads are the offsets plus constants (component blocks of
-// kTlPlane entries, rows of kTlBoxX).  Dead links of the direction were
-// zeroed in the staged boxes, so every read is a plain shared-memory load.
+// neighbour reads are the offsets plus constants (component blocks of kPlane
+// entries, rows of kBoxX).  Dead links of the direction were zeroed in the
+// staged boxes, so every read is a plain shared-memory load.
+template <int NX>
 struct TlNb {
+  using S = TlShape<NX>;
   int lo, mid, hi;
   __device__ __forceinline__ int at(int di, int dj, int dk) const {
-    return (dk < 0 ? lo : (dk > 0 ? hi : mid)) + di + dj * kTlBoxX;
+    return (dk < 0 ? lo : (dk > 0 ? hi : mid)) + di + dj * S::kBoxX;
   }
   __device__ __forceinline__ void psi(int di, int dj, int dk, float& re, float& im) const {
     const int e = at(di, dj, dk);
     re = tl_smem[e];
-    im = tl_smem[e + kTlPlane];
+    im = tl_smem[e + S::kPlane];
   }
   __device__ __forceinline__ float phi(int a, int di, int dj, int dk) const {
-    return tl_smem[at(di, dj, dk) + (2 + a) * kTlPlane];
+    return tl_smem[at(di, dj, dk) + (2 + a) * S::kPlane];
   }
 };
 
@@ -147,8 +162,9 @@ struct TlNb {
 // offsets, in float).
 __device__ __forceinline__ void tl_store(const Grid& g, float* E, long npf, long m, int i, int j, int k, bool face,
                                          const float* v) {
+  float* e = E + m;
 #pragma unroll
-  for (int c = 0; c < kTlComp; ++c) E[c * npf + m] = v[c];
+  for (int c = 0; c < kTlComp; ++c, e += npf) *e = v[c];
   if (!face) return;
   const float tx = (i == g.Nx - 1) ? 0.0f : v[2];
   const float ty = (j == g.Ny - 1) ? 0.0f : v[3];
@@ -184,33 +200,38 @@ __device__ __forceinline__ void tl_store(const Grid& g, float* E, long npf, long
   }
 }
 
-// Zero the dead links at box position o of a staged direction (link bits b);
-// raw (may be null) receives the three raw link values first.
+// Zero the dead links (bits b) at entry offset o of a staged direction box of
+// kPlane entries per component; raw (may be null) receives the three raw link
+// values first.
+template <int PLANE>
 __device__ __forceinline__ void tl_fix(float* P, int o, uint32_t b, float* raw) {
   if (raw) {
-    raw[0] = P[2 * kTlPlane + o];
-    raw[1] = P[3 * kTlPlane + o];
-    raw[2] = P[4 * kTlPlane + o];
+    raw[0] = P[2 * PLANE + o];
+    raw[1] = P[3 * PLANE + o];
+    raw[2] = P[4 * PLANE + o];
   }
-  if (b & 1u) P[2 * kTlPlane + o] = 0.0f;
-  if (b & 2u) P[3 * kTlPlane + o] = 0.0f;
-  if (b & 4u) P[4 * kTlPlane + o] = 0.0f;
+  if (b & 1u) P[2 * PLANE + o] = 0.0f;
+  if (b & 2u) P[3 * PLANE + o] = 0.0f;
+  if (b & 4u) P[4 * PLANE + o] = 0.0f;
 }
 
-// Product (POLY false) or Horner step (POLY true) over a 32 x 8 tile and the
-// planes of chunk blockIdx.z.  Grid: (ceil(nx / 32), ceil(ny / 8), chunks),
-// chunks <= nz; kThreads threads; kTlSmem bytes of dynamic shared memory.
+// Product (POLY false) or Horner step (POLY true) over a (32 NX) x 8 tile and
+// the planes of chunk blockIdx.z.  Grid: (ceil(nx / (32 NX)), ceil(ny / 8),
+// chunks), chunks <= nz; kThreads threads; TlShape<NX>::kSmem bytes of
+// dynamic shared memory.
 //
-// Staged plane q (z = k0 - 1 + q) goes to slot q % kTlSlots.  Iteration p
-// (plane k = k0 - 1 + p) waits for staged plane p + 1, zeroes its dead links
-// (each thread its own box position, threads 0..83 one position of the box's
-// ring each), passes the block barrier, lets thread 0 issue staged plane p + 3
-// into the slot of plane p - 2 (every thread is past iteration p - 1, the last
+// Staged plane q (z = k0 - 1 + q) goes to slot q % kSlots.  Iteration p
+// (plane k = k0 - 1 + p) waits for staged plane p + 1, zeroes its dead links,
+// passes the block barrier, lets thread 0 issue staged plane p + kAhead into
+// the slot of plane p - 2 (every thread is past iteration p - 1, the last
 // reader of that slot), and computes plane k from the slots of p - 1, p, p + 1.
-template <bool POLY>
-__global__ void __launch_bounds__(kThreads, TDGL_TL_MINB) kg_tl(const __grid_constant__ TlMaps M, GArgs<float> A) {
+template <bool POLY, int NX>
+__global__ void __launch_bounds__(kThreads, TlShape<NX>::kMinBlocks)
+    kg_tl(const __grid_constant__ TlMaps M, GArgs<float> A) {
+  using S = TlShape<NX>;
+  constexpr int SL = S::kSlots, SF = S::kSlotF, PL = S::kPlane, BX = S::kBoxX;
   float* const tsm = tl_smem;
-  __shared__ __align__(8) uint64_t bar[kTlSlots];
+  __shared__ __align__(8) uint64_t bar[SL];
   GDev* d = A.dev;
   if (!gdev_ok(d)) return;
   if (POLY && A.pmode) {
@@ -258,75 +279,88 @@ __global__ void __launch_bounds__(kThreads, TDGL_TL_MINB) kg_tl(const __grid_con
   const int k0 = 1 + (int)(((long)blockIdx.z * g.nz) / nch);
   const int k1 = (int)(((long)(blockIdx.z + 1) * g.nz) / nch);
   const int nq = k1 - k0 + 3;
-  const int bx = blockIdx.x * kTlTx, by = blockIdx.y * kTlTy;   // box origin: (i0 - 1, j0 - 1)
+  const int bx = blockIdx.x * S::kTx, by = blockIdx.y * kTlTy;   // box origin: (i0 - 1, j0 - 1)
   const CUtensorMap* mx = &M.m[TM_X];
   const CUtensorMap* mp = &M.m[pm];
   const bool p5 = pm == TM_UB;
   int issued = 0;                                  // thread 0: staged planes issued so far
-  auto issue = [&](int q) {                        // staged plane q into slot q % kTlSlots
-    const int s = q % kTlSlots;
-    float* dx = tsm + (size_t)s * 2 * kTlSlotF;
+  auto issue = [&](int q) {                        // staged plane q into slot q % SL
+    const int s = q % SL;
+    float* dx = tsm + (size_t)s * 2 * SF;
     const int z = k0 - 1 + q;
     fence_proxy_async_smem();                      // the block's earlier writes to this slot come first
-    mbar_expect_tx(&bar[s], 2 * kTlBytes);
+    mbar_expect_tx(&bar[s], 2 * S::kBytes);
     tma_load4(dx, mx, bx, by, z, 0, &bar[s]);
-    if (p5) tma_load5(dx + kTlSlotF, mp, bx, by, z, 0, ja, &bar[s]);
-    else tma_load4(dx + kTlSlotF, mp, bx, by, z, 0, &bar[s]);
+    if (p5) tma_load5(dx + SF, mp, bx, by, z, 0, ja, &bar[s]);
+    else tma_load4(dx + SF, mp, bx, by, z, 0, &bar[s]);
     ++issued;
   };
   if (threadIdx.x == 0) {
-    for (int s = 0; s < kTlSlots; ++s) mbar_init(&bar[s], 1);
+    for (int s = 0; s < SL; ++s) mbar_init(&bar[s], 1);
     mbar_fence_init();
   }
   __syncthreads();
   if (threadIdx.x == 0)
-    for (int q = 0; q < kTlSlots - 1 && q < nq; ++q) issue(q);
+    for (int q = 0; q <= S::kAhead && q < nq; ++q) issue(q);
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-  const int i = 1 + bx + tx, j = 1 + by + ty;
-  const bool act = i <= g.nx && j <= g.ny;
-  const int o = (ty + 1) * kTlBoxX + (tx + 1);
-  // box positions whose dead links this thread zeroes: its own (when on the
-  // full grid) and, for threads 0..83, one of the ring around the tile
-  const bool own_in = i <= g.Nx && j <= g.Ny;
+  const int j = 1 + by + ty;
+  int iu[NX], ou[NX];
+  bool act[NX], own_in[NX];
+  long om[NX];
+#pragma unroll
+  for (int u = 0; u < NX; ++u) {
+    iu[u] = 1 + bx + tx + 32 * u;
+    act[u] = iu[u] <= g.nx && j <= g.ny;
+    own_in[u] = iu[u] <= g.Nx && j <= g.Ny;      // on the full grid: its dead links are zeroed
+    ou[u] = (ty + 1) * BX + (tx + 1 + 32 * u);
+    om[u] = (long)iu[u] + (long)g.mj * j;        // full-grid index in plane 0
+  }
+  // one position of the ring around the tile (threads 0 .. kRing - 1)
   int ho = -1;
   long hm = 0;
   {
-    const int t = threadIdx.x;
+    const int t = threadIdx.x, w = S::kTx + 2;
     int hx = -1, hy = -1;
-    if (t < 34) hx = t, hy = 0;
-    else if (t < 68) hx = t - 34, hy = kTlBoxY - 1;
-    else if (t < 76) hx = 0, hy = 1 + (t - 68);
-    else if (t < 84) hx = kTlTx + 1, hy = 1 + (t - 76);
+    if (t < w) hx = t, hy = 0;
+    else if (t < 2 * w) hx = t - w, hy = kTlBoxY - 1;
+    else if (t < 2 * w + kTlTy) hx = 0, hy = 1 + (t - 2 * w);
+    else if (t < S::kRing) hx = S::kTx + 1, hy = 1 + (t - 2 * w - kTlTy);
     if (hx >= 0 && bx + hx <= g.Nx && by + hy <= g.Ny) {
-      ho = hy * kTlBoxX + hx;
+      ho = hy * BX + hx;
       hm = (long)(bx + hx) + (long)g.mj * (by + hy);
     }
   }
-  const long om = (long)i + (long)g.mj * j;        // own position's full-grid index in plane 0
-  auto dead_bits = [&](int q) -> uint32_t {        // own bits | ring bits << 8 of staged plane q
+  auto dead_bits = [&](int q) -> uint32_t {        // own bits << 4 u | ring bits << 16 of staged plane q
     const long zb = (long)g.mk * (k0 - 1 + q);
-    uint32_t b = own_in ? (uint32_t)__ldg(A.ldead + zb + om) : 0u;
-    if (ho >= 0) b |= (uint32_t)__ldg(A.ldead + zb + hm) << 8;
+    uint32_t b = 0u;
+#pragma unroll
+    for (int u = 0; u < NX; ++u)
+      if (own_in[u]) b |= (uint32_t)__ldg(A.ldead + zb + om[u]) << (4 * u);
+    if (ho >= 0) b |= (uint32_t)__ldg(A.ldead + zb + hm) << 16;
     return b;
   };
-  auto fix = [&](int q, uint32_t b, float* raw) {
-    float* P = tsm + (size_t)(q % kTlSlots) * 2 * kTlSlotF + kTlSlotF;
-    if (own_in) tl_fix(P, o, b, raw);
-    if (ho >= 0) tl_fix(P, ho, b >> 8, nullptr);
+  auto fix = [&](int q, uint32_t b, float (*raw)[3]) {
+    float* P = tsm + (size_t)(q % SL) * 2 * SF + SF;
+#pragma unroll
+    for (int u = 0; u < NX; ++u)
+      if (own_in[u]) tl_fix<PL>(P, ou[u], b >> (4 * u), raw ? raw[u] : nullptr);
+    if (ho >= 0) tl_fix<PL>(P, ho, b >> 16, nullptr);
   };
   auto aborted = [&](bool ok) -> bool {            // block-wide: a wait ran out
     if (!__syncthreads_or(!ok)) return false;
     // wait (bounded) for every copy still in flight into this block's shared
     // memory, record the status, stop
     if (threadIdx.x == 0) {
-      for (int q = issued > kTlSlots ? issued - kTlSlots : 0; q < issued; ++q)
-        mbar_wait(&bar[q % kTlSlots], (unsigned)((q / kTlSlots) & 1), kTlDrainNs);
+      for (int q = issued > SL ? issued - SL : 0; q < issued; ++q)
+        mbar_wait(&bar[q % SL], (unsigned)((q / SL) & 1), kTlDrainNs);
       atomicCAS(&d->status, GS_OK, GS_TIMEOUT);
     }
     return true;
   };
   // staged planes 0 and 1 (k0 - 1, k0) before the loop
-  float raw[3] = {0.0f, 0.0f, 0.0f}, raw_next[3];
+  float raw[NX][3], raw_next[NX][3];
+#pragma unroll
+  for (int u = 0; u < NX; ++u) raw[u][0] = raw[u][1] = raw[u][2] = 0.0f;
   bool ok = mbar_wait(&bar[0], 0u, wait_ns);
   if (ok) fix(0, dead_bits(0), nullptr);
   ok = ok && mbar_wait(&bar[1], 0u, wait_ns);
@@ -338,63 +372,83 @@ __global__ void __launch_bounds__(kThreads, TDGL_TL_MINB) kg_tl(const __grid_con
   // data and store nothing.
   const int dn = g.nx * g.ny;
   const long dmk = g.mk;
-  int n = act ? dix(g, i, j, k0) : 0;
-  long m = act ? full_index(g, i, j, k0) : full_index(g, 1, 1, k0);
-  const bool face_ij = i == 1 || i == g.Nx - 1 || j == 1 || j == g.Ny - 1;
-  const float cx = (float)A.cxu, cy = (float)A.cyu, cz = (float)A.czu;
-  const bool material = g.has_material != 0;
-  uint8_t nf = g.nflags[n];
-  float v[5] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
-  if (POLY && Vg) {
+  int n[NX];
+  long m[NX];
+  bool face_ij[NX];
+  uint8_t nf[NX];
+  float v[NX][5];
 #pragma unroll
-    for (int c = 0; c < kTlComp; ++c) v[c] = __ldg(Vg + c * npf + m);
+  for (int u = 0; u < NX; ++u) {
+    n[u] = act[u] ? dix(g, iu[u], j, k0) : 0;
+    m[u] = act[u] ? full_index(g, iu[u], j, k0) : full_index(g, 1, 1, k0);
+    face_ij[u] = iu[u] == 1 || iu[u] == g.Nx - 1 || j == 1 || j == g.Ny - 1;
+    nf[u] = g.nflags[n[u]];
+#pragma unroll
+    for (int c = 0; c < kTlComp; ++c) v[u][c] = (POLY && Vg) ? __ldg(Vg + c * npf + m[u]) : 0.0f;
   }
+  const float cx = (float)A.cxu, cy = (float)A.cyu, cz = (float)A.czu;
+  const float ihx = (float)g.ihx2, ihy = (float)g.ihy2, ihz = (float)g.ihz2;
+  const bool material = g.has_material != 0;
   for (int k = k0; k <= k1; ++k) {
     const int p = k - k0 + 1;                      // staged index of plane k
-    ok = ok && mbar_wait(&bar[(p + 1) % kTlSlots], (unsigned)(((p + 1) / kTlSlots) & 1), wait_ns);
+    ok = ok && mbar_wait(&bar[(p + 1) % SL], (unsigned)(((p + 1) / SL) & 1), wait_ns);
     if (ok) fix(p + 1, db_next, raw_next);
     if (aborted(ok)) return;
-    if (threadIdx.x == 0 && p + 3 < nq) issue(p + 3);
+    if (threadIdx.x == 0 && p + S::kAhead < nq) issue(p + S::kAhead);
     if (p + 2 < nq) db_next = dead_bits(p + 2);
     const bool more = k < k1;
-    const uint8_t nf_next = more ? g.nflags[n + dn] : (uint8_t)0;
-    float v_next[5] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
-    if (POLY && Vg && more) {
+    uint8_t nf_next[NX];
+    float v_next[NX][5];
 #pragma unroll
-      for (int c = 0; c < kTlComp; ++c) v_next[c] = __ldg(Vg + c * npf + m + dmk);
+    for (int u = 0; u < NX; ++u) {
+      nf_next[u] = more ? g.nflags[n[u] + dn] : (uint8_t)0;
+#pragma unroll
+      for (int c = 0; c < kTlComp; ++c)
+        v_next[u][c] = (POLY && Vg && more) ? __ldg(Vg + c * npf + m[u] + dmk) : 0.0f;
     }
-    NodeCoef<float> nc;
-    if (g.kappa_per_node) {
-      nc = node_coef<float>(g, n, nf);
-    } else {
-      nc.cx = cx; nc.cy = cy; nc.cz = cz;
-      nc.material = material;
-      nc.sc = (material && (nf & NF_SCFRAC)) ? (float)g.scint[n] : ((material && (nf & NF_SC0)) ? 0.0f : 1.0f);
+    const int s0 = (p % SL) * 2 * SF, sm = ((p - 1) % SL) * 2 * SF, sp = ((p + 1) % SL) * 2 * SF;
+#pragma unroll
+    for (int u = 0; u < NX; ++u) {
+      NodeCoef<float> nc;
+      if (g.kappa_per_node) {
+        nc = node_coef<float>(g, n[u], nf[u]);
+      } else {
+        nc.cx = cx; nc.cy = cy; nc.cz = cz;
+        nc.material = material;
+        nc.sc = (material && (nf[u] & NF_SCFRAC)) ? (float)g.scint[n[u]]
+                                                  : ((material && (nf[u] & NF_SC0)) ? 0.0f : 1.0f);
+        nc.ihx = ihx; nc.ihy = ihy; nc.ihz = ihz;
+      }
+      const int b0 = s0 + ou[u], bm = sm + ou[u], bp = sp + ou[u];
+      const TlNb<NX> X{bm, b0, bp};
+      const TlNb<NX> P{bm + SF, b0 + SF, bp + SF};
+      float r[5];
+      jvp_body<float, true>(g, X, P, nc, nf[u], r);
+      // the direction's raw values at the node: psi from the box, links saved before zeroing
+      const float w[5] = {tl_smem[b0 + SF], tl_smem[b0 + SF + PL], raw[u][0], raw[u][1], raw[u][2]};
+      float z[5];
+#pragma unroll
+      for (int c = 0; c < kTlComp; ++c) z[c] = fmaf(cr, r[c], fmaf(cw, w[c], cv * v[u][c]));
+      if (act[u]) tl_store(g, out, npf, m[u], iu[u], j, k, face_ij[u] || k == 1 || k == g.Nz - 1, z);
     }
-    const int b0 = (p % kTlSlots) * 2 * kTlSlotF + o;
-    const int bm = ((p - 1) % kTlSlots) * 2 * kTlSlotF + o;
-    const int bp = ((p + 1) % kTlSlots) * 2 * kTlSlotF + o;
-    const TlNb X{bm, b0, bp};
-    const TlNb P{bm + kTlSlotF, b0 + kTlSlotF, bp + kTlSlotF};
-    float r[5];
-    jvp_body<float, true>(g, X, P, nc, nf, r);
-    // the direction's raw values at the node: psi from the box, links saved before zeroing
-    const float w[5] = {tl_smem[b0 + kTlSlotF], tl_smem[b0 + kTlSlotF + kTlPlane], raw[0], raw[1], raw[2]};
-    float z[5];
 #pragma unroll
-    for (int c = 0; c < kTlComp; ++c) z[c] = fmaf(cr, r[c], fmaf(cw, w[c], cv * v[c]));
-    if (act) tl_store(g, out, npf, m, i, j, k, face_ij || k == 1 || k == g.Nz - 1, z);
+    for (int u = 0; u < NX; ++u) {
 #pragma unroll
-    for (int c = 0; c < 3; ++c) raw[c] = raw_next[c];
-    nf = nf_next;
+      for (int c = 0; c < 3; ++c) raw[u][c] = raw_next[u][c];
+      nf[u] = nf_next[u];
 #pragma unroll
-    for (int c = 0; c < kTlComp; ++c) v[c] = v_next[c];
-    if (act) {
-      n += dn;
-      m += dmk;
+      for (int c = 0; c < kTlComp; ++c) v[u][c] = v_next[u][c];
+      if (act[u]) {
+        n[u] += dn;
+        m[u] += dmk;
+      }
     }
   }
   kt_end(d, KT_ARN_APPLY);
 }
 
+}  // namespace tdgl
+
+namespace tdgl {
+inline size_t tl_smem_bytes(int NX) { return NX == 2 ? TlShape<2>::kSmem : TlShape<1>::kSmem; }
 }  // namespace tdgl

@@ -243,8 +243,15 @@ class DeviceGrid:
                                           C.byref(opts), C.byref(field), C.c_void_p(stream.cuda_stream)),
                 "tdgl_trap_launch")
 
+    def trap_launch_next(self, x: torch.Tensor, max_steps: int, opts: L.TrapOpts, field: L.Field,
+                         stream: torch.cuda.Stream) -> None:
+        """Enqueue up to max_steps more steps continuing from the clock and state
+        the previous launch leaves on the device (returns at once)."""
+        L.check(self.lib.tdgl_trap_launch_next(self.handle, _ptr(x), int(max_steps), C.byref(opts), C.byref(field),
+                                               C.c_void_p(stream.cuda_stream)), "tdgl_trap_launch_next")
+
     def trap_collect(self) -> tuple[int, float, float, dict]:
-        """Results of the last trap_launch (its stream must have completed)."""
+        """Results of the oldest queued launch (waits for it)."""
         tt, dd = C.c_double(0.0), C.c_double(0.0)
         st = L.Stats()
         rc = self.lib.tdgl_trap_collect(self.handle, C.byref(tt), C.byref(dd), C.byref(st))

@@ -279,51 +279,69 @@ def _count_steps(t_start: float, t_stop: float, dt: float) -> int:
 class _History:
     """Saved states on their way to host memory while the device steps on.
 
-    save(x): the state is unpacked into one of two device staging buffers on
-    the compute stream (before the next launch changes x), copied
-    asynchronously on a side stream into pinned host staging, and a worker
-    thread copies it into row k of the output (preallocated for the expected
-    number of saves; rows beyond it, after dt retries, are appended).  The
-    host copy runs as several memmove calls on a small thread pool: they
+    stage(x): the state is unpacked into one of NBUF device staging buffers on
+    the compute stream (in stream order, before a later launch changes x) and
+    copied asynchronously on a side stream into pinned host staging; the
+    token it returns is then either committed as row k of the output (a
+    worker thread copies it there once the copy has landed) or discarded.
+    save(x) stages and commits at once.  The output is preallocated for the
+    expected number of saves; rows beyond it, after dt retries, are appended.
+    The host copy runs as several memmove calls on a small thread pool: they
     release the GIL (a torch CPU copy holds it, stalling the stepping thread
     for its whole duration) and share the page faults of the fresh output
-    rows.  The host-side copies overlap the next device launch.
+    rows.  The host-side copies overlap the next device launches.
     """
 
     COPY_THREADS = max(1, min(8, (os.cpu_count() or 1) // 2))
+    NBUF = 3
 
     def __init__(self, g, rows: int):
         self.g = g
         self.rows = torch.empty((max(rows, 1), g.n_state), dtype=torch.complex128)
         self.extra: list[torch.Tensor] = []
         self.n = 0
+        self.nstaged = 0
         st = getattr(g, "_history_staging", None)
-        if st is None:
-            st = {"dev": [torch.empty(g.n_state, dtype=torch.complex128, device=g.device) for _ in range(2)],
-                  "pin": [torch.empty(g.n_state, dtype=torch.complex128, pin_memory=True) for _ in range(2)],
+        if st is None or len(st["dev"]) < self.NBUF:
+            st = {"dev": [torch.empty(g.n_state, dtype=torch.complex128, device=g.device) for _ in range(self.NBUF)],
+                  "pin": [torch.empty(g.n_state, dtype=torch.complex128, pin_memory=True)
+                          for _ in range(self.NBUF)],
                   "stream": torch.cuda.Stream(device=g.device)}
             g._history_staging = st
         self.st = st
-        self.ready = [torch.cuda.Event() for _ in range(2)]
-        self.copied = [torch.cuda.Event() for _ in range(2)]
-        self.futs = [None, None]
+        self.ready = [torch.cuda.Event() for _ in range(self.NBUF)]
+        self.copied = [torch.cuda.Event() for _ in range(self.NBUF)]
+        self.futs = [None] * self.NBUF
         self.pool = ThreadPoolExecutor(max_workers=1)
         self.copy_pool = ThreadPoolExecutor(max_workers=self.COPY_THREADS)
         self.lock = threading.Lock()
 
-    def save(self, x: torch.Tensor) -> None:
-        k = self.n % 2
+    def stage(self, x: torch.Tensor) -> int:
+        k = self.nstaged % self.NBUF
+        self.nstaged += 1
         if self.futs[k] is not None:
             self.futs[k].result()
+            self.futs[k] = None
         st = self.st
+        # the side-stream copy of this buffer's previous state (kept or not) reads dev[k]
+        torch.cuda.current_stream(self.g.device).wait_event(self.copied[k])
         self.g.unpack(x, out=st["dev"][k])
         self.ready[k].record()
         with torch.cuda.stream(st["stream"]):
             st["stream"].wait_event(self.ready[k])
             st["pin"][k].copy_(st["dev"][k], non_blocking=True)
             self.copied[k].record(st["stream"])
+        return k
+
+    def commit(self, k: int) -> None:
         self.futs[k] = self.pool.submit(self._land, k, self.n)
         self.n += 1
+
+    def discard(self, k: int) -> None:
+        """The staged state is not kept (the buffer is free once its copy has run)."""
+
+    def save(self, x: torch.Tensor) -> None:
+        self.commit(self.stage(x))
 
     def _copy(self, dst: torch.Tensor, src: torch.Tensor) -> None:
         nbytes = src.numel() * src.element_size()
@@ -352,6 +370,8 @@ class _History:
         for f in self.futs:
             if f is not None:
                 f.result()
+        torch.cuda.current_stream(self.g.device).synchronize()
+        self.st["stream"].synchronize()
         self.pool.shutdown(wait=True)
         self.copy_pool.shutdown(wait=True)
         if not self.extra and self.n == self.rows.shape[0]:
@@ -366,6 +386,75 @@ def _field_at(eval_u, t, params, idx) -> L.Field:
     return L.Field(bx, by, bz, 1.0, 0.5, 1.0, 0, 1)
 
 
+def _add_counts(tot: dict, st: dict) -> None:
+    for k in tot:
+        tot[k] = max(tot[k], st[k]) if k == "max_krylov" else tot[k] + (1 if k == "kernel_launches" else st[k])
+
+
+def _check_step(rc: int, t: float, cur: float, t_stop: float, dt_min: float) -> None:
+    """The integrator's failures as the reference reports them
+    (integrators.py:186-197); other device statuses as TDGLError."""
+    if rc == L.TDGL_ENOCONV:
+        raise RuntimeError(f"Newton did not converge at t={t:.6e} with dt={min(cur, t_stop - t):.3e}.")
+    if rc == L.TDGL_EDTMIN:
+        raise RuntimeError(f"dt reduced below dt_min={dt_min:.1e} at t={t:.6e}; aborting.")
+    L.check(rc, "tdgl_trap_run")
+
+
+def _clock_after(t: float, dt: float, t_stop: float, n: int) -> float:
+    """The clock after n accepted steps of min(dt, t_stop - t) (no retries)."""
+    for _ in range(n):
+        if not t < t_stop - 1e-14:
+            break
+        t += min(dt, t_stop - t)
+    return t
+
+
+def _trap_queued(g, x, t, cur, t_stop, dt, save_every, opts, field, hist, times, tot, dt_min, verbose):
+    """The step loop of trapezoidal with the next launch queued on the device
+    before the previous one is collected (tdgl_trap_launch_next continues
+    from the clock the previous launch leaves), so the GPU steps on while the
+    host reads a launch's counters and lands its state.  Each launch makes up
+    to save_every accepted steps; its state is staged right behind it in
+    stream order and kept when the reference would save it
+    (integrators.py:180-182).  A launch is queued while the clock predicted
+    without retries is short of t_stop, and again whenever the queue has run
+    dry before t_stop (after dt retries).  Returns (t, dt_cur, steps)."""
+    stream = torch.cuda.current_stream(g.device)
+    queue = []
+    g.trap_launch(x, t, cur, save_every, opts, field, stream)
+    queue.append(hist.stage(x))
+    t_pred = _clock_after(t, dt, t_stop, save_every)
+    step = 0
+    while queue:
+        if len(queue) < 2 and t_pred < t_stop - 1e-14:
+            g.trap_launch_next(x, save_every, opts, field, stream)
+            queue.append(hist.stage(x))
+            t_pred = _clock_after(t_pred, dt, t_stop, save_every)
+        rc, t, cur, st = g.trap_collect()
+        k = queue.pop(0)
+        _add_counts(tot, st)
+        step += st["steps"]
+        if rc != L.TDGL_OK:
+            while queue:                     # the queued continuation is drained, its result dropped
+                g.trap_collect()
+                hist.discard(queue.pop(0))
+            hist.discard(k)
+            _check_step(rc, t, cur, t_stop, dt_min)
+        if verbose:
+            print(f"  t={t:.4f} steps={step} newton={st['newton_iters']} krylov={st['krylov_iters']}")
+        if st["steps"] > 0 and step % save_every == 0:
+            times.append(t)
+            hist.commit(k)
+        else:
+            hist.discard(k)
+        if not queue and t < t_stop - 1e-14:
+            g.trap_launch_next(x, save_every, opts, field, stream)
+            queue.append(hist.stage(x))
+            t_pred = _clock_after(t, dt, t_stop, save_every)
+    return t, cur, step
+
+
 def trapezoidal(x0, params, idx, eval_u: Callable, t_start: float, t_stop: float, dt: float, *,
                 newton_tol_f: float = 1e-3, newton_tol_dx: float = 1e-3, newton_max_iter: int = 20,
                 tol_gcr: float = 1e-4, eps_mf: float = 1e-4, save_every: int = 1, adaptive: bool = True,
@@ -377,9 +466,11 @@ def trapezoidal(x0, params, idx, eval_u: Callable, t_start: float, t_stop: float
     shape (n_state, n_saved), as the reference does.
 
     The step loop, Newton and Krylov iterations and the retries run inside one
-    device launch per saved state; the host only stores saved states.  With an
-    ``eval_u`` the device cannot evaluate (a Python ``field_func``), one launch
-    per step is made with the field evaluated on the host at the step's start.
+    device launch per saved state; the host only stores saved states, and
+    with the GMRES executor the next launch is queued before the previous one
+    is collected.  With an ``eval_u`` the device cannot evaluate (a Python
+    ``field_func``), one launch per step is made with the field evaluated on
+    the host at the step's start.
     """
     jvp = jvp or ("fd" if precision == "fp64" else "analytic")
     g = grid_for(params, idx, material, precision, kmax, default_krylov(krylov, jvp))
@@ -397,19 +488,17 @@ def trapezoidal(x0, params, idx, eval_u: Callable, t_start: float, t_stop: float
     tot = {"steps": 0, "newton_iters": 0, "krylov_iters": 0, "rhs_evals": 0, "jvp_evals": 0, "rejections": 0,
            "max_krylov": 0, "kernel_launches": 0}
     step = 0
+    if dev_field is not None and g.krylov == "gmres" and t < t_stop - 1e-14:
+        t, cur, step = _trap_queued(g, x, t, cur, float(t_stop), float(dt), max(int(save_every), 1), opts, dev_field,
+                                    hist, times, tot, float(dt_min), verbose)
     while t < t_stop - 1e-14:
         if dev_field is not None:
             rc, t, cur, st = g.trap_run(x, t, cur, int(save_every), opts, dev_field)
         else:
             rc, t, cur, st = g.trap_run(x, t, cur, 1, opts, _field_at(eval_u, t, params, idx))
-        for k in tot:
-            tot[k] = max(tot[k], st[k]) if k == "max_krylov" else tot[k] + (1 if k == "kernel_launches" else st[k])
+        _add_counts(tot, st)
         step += st["steps"]
-        if rc == L.TDGL_ENOCONV:
-            raise RuntimeError(f"Newton did not converge at t={t:.6e} with dt={min(cur, t_stop - t):.3e}.")
-        if rc == L.TDGL_EDTMIN:
-            raise RuntimeError(f"dt reduced below dt_min={dt_min:.1e} at t={t:.6e}; aborting.")
-        L.check(rc, "tdgl_trap_run")
+        _check_step(rc, t, cur, t_stop, dt_min)
         if verbose:
             print(f"  t={t:.4f} steps={step} newton={st['newton_iters']} krylov={st['krylov_iters']}")
         if st["steps"] > 0 and step % save_every == 0:

@@ -9,8 +9,9 @@ the product kernel, interior entries back).
 * Mixed contexts (FP32 vectors; the TMA-staged kernel on 3-D grids) against
   the FP64 product: 2e-6 relative to max |ap| (FP32 rounding of the inputs and
   the stencil).
-* The TMA-staged kernel against the FP32 kernel that reads global memory
-  (TDGL_TMA=0): 1e-6 relative (same arithmetic, contraction order may differ).
+* The TMA-staged kernel (one and two nodes per thread, TDGL_TL_NX) against
+  the FP32 kernel that reads global memory (TDGL_TMA=0): 1e-6 relative (same
+  arithmetic, contraction order may differ).
 * z-chunking of the TMA-staged kernel (TDGL_TL_CHUNKS): bit-identical outputs
   for every chunk count.
 * The 128x128x32 bench device (4 x 16 tiles per plane, the hole): FP32 against
@@ -94,25 +95,28 @@ def _tiled_device(tb, periodic=(False, False, False)):
     return dev
 
 
+@pytest.mark.parametrize("nx", ["1", "2"])
 @pytest.mark.parametrize("periodic", [(False, False, False), (True, True, True)])
-def test_tma_kernel_against_global_memory_kernel(monkeypatch, periodic):
+def test_tma_kernel_against_global_memory_kernel(monkeypatch, periodic, nx):
     import nanowire_tdgl_b200 as tb
     dev = _tiled_device(tb, periodic)
     X, P = _state_and_direction(dev, 5)
     B = (0.05, 0.1, 0.4)
-    tma, want = _products(dev, X, P, B, "mixed")
+    tma, want = _products(dev, X, P, B, "mixed", {"TDGL_TL_NX": nx}, monkeypatch)
     plain, _ = _products(dev, X, P, B, "mixed", {"TDGL_TMA": "0"}, monkeypatch)
     assert _rel(tma, want) < 2e-6
     assert _rel(plain, want) < 2e-6
     assert _rel(tma, plain) < 1e-6
 
 
-def test_tma_chunks_are_bit_identical(monkeypatch):
+@pytest.mark.parametrize("nx", ["1", "2"])
+def test_tma_chunks_are_bit_identical(monkeypatch, nx):
     import nanowire_tdgl_b200 as tb
     dev = _tiled_device(tb)
     X, P = _state_and_direction(dev, 6)
     B = (0.0, 0.0, 0.4)
-    outs = [_products(dev, X, P, B, "mixed", {"TDGL_TL_CHUNKS": str(c)}, monkeypatch)[0] for c in (1, 2, 4, 11)]
+    outs = [_products(dev, X, P, B, "mixed", {"TDGL_TL_CHUNKS": str(c), "TDGL_TL_NX": nx}, monkeypatch)[0]
+            for c in (1, 2, 4, 11)]
     for o in outs[1:]:
         assert np.array_equal(o, outs[0])
 
