@@ -43,10 +43,14 @@ WORKLOAD_NAME = ("trapezoidal step, 128x128x32-cell film (499,999 interior nodes
 HBM_FALLBACK_GBS = 6650.0
 WORKLOAD_N_INTERIOR = 127 * 127 * 31
 # DRAM bytes per algorithmic byte of the GMRES step graph on the 128x128x32
-# workload (degree-3 preconditioner), from a graph-level ncu capture of a
-# 2-step launch: 6.49 GB DRAM against 15.0 GB algorithmic.  The preconditioned
-# solves keep their basis (<= 10 vectors, 110 MB) in L2.
-DRAM_PER_ALG_BYTE = 0.432
+# workload at the default preconditioner degree (5), from a graph-level ncu
+# capture (dram__bytes_read.sum + dram__bytes_write.sum) of the timed 2-step
+# launch of `bench.py --steps 2 --warmup 3 --no-fp64 --no-e2e
+# --no-cpu-baseline --no-forms`: 1.299 GB read + 1.992 GB written = 3.291 GB
+# against 13.317 GB algorithmic.  The preconditioned solves keep their basis
+# (<= 7 vectors of 11 MB) and the stencil vectors in L2.
+DRAM_PER_ALG_BYTE = 0.2471
+DRAM_RATIO_DEGREE = 5
 
 
 def parse():
@@ -61,11 +65,15 @@ def parse():
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison run")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-forms", action="store_true",
+                    help="skip the other forms (trilayer, batched, differentiation) after the headline line")
     ap.add_argument("--cpu-budget-s", type=float, default=150.0)
     ap.add_argument("--form", choices=["precision", "adjoint", "batched", "trilayer"], default="precision",
                     help="adjoint: gradients of the 64x64x16 differentiation workload; batched: instance-steps/s "
                          "of 64 uneven instances stepped together against looping them (--steps per instance); "
                          "trilayer: the 256x256x64 S/I/S stack, mixed against FP64")
+    ap.add_argument("--adj-smax", type=float, default=ADJ["s_max"],
+                    help="upper end of the suppression field s(x) of the differentiation workload")
     ap.add_argument("--arnoldi-probe", type=int, default=None, metavar="J",
                     help="diagnostic: time the three Arnoldi-step kernels standalone at basis index J and exit")
     ap.add_argument("--kernel-timers", action="store_true",
@@ -299,11 +307,12 @@ def run_ours(a, rank, world):
     # launch of this workload in mixed precision at the default preconditioner
     # degree; traffic follows the Krylov counters, so it is scaled by this
     # run's algorithmic bytes (reported only at that degree).
-    traffic = (DRAM_PER_ALG_BYTE * alg if (a.precision == "mixed" and a.krylov == "gmres" and poly_deg == 3)
-               else None)
-    traffic_note = (None if traffic is not None else
-                    "not captured at this configuration (the DRAM/algorithmic ratio 0.432 was measured with ncu at "
-                    "preconditioner degree 3; a higher degree keeps an even smaller basis in L2)")
+    traffic = (DRAM_PER_ALG_BYTE * alg
+               if (a.precision == "mixed" and a.krylov == "gmres" and poly_deg == DRAM_RATIO_DEGREE) else None)
+    traffic_note = (f"{DRAM_PER_ALG_BYTE} x the algorithmic bytes: the DRAM/algorithmic ratio of a graph-level ncu "
+                    "capture of this workload's timed launch at this configuration" if traffic is not None else
+                    f"not captured at this configuration (the ratio {DRAM_PER_ALG_BYTE} is for mixed precision, "
+                    f"GMRES, preconditioner degree {DRAM_RATIO_DEGREE})")
     out = {
         "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "weak",
@@ -320,6 +329,11 @@ def run_ours(a, rank, world):
         "gpu_launches": graph_launches(st, jvp, poly_deg) if a.krylov == "gmres" else 1,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "traffic_note": traffic_note, "peak_kind": peak_kind,
+                     "limiter": ("the roofline is HBM (streaming stencils, no contraction), but the preconditioned "
+                                 "step's working set stays in L2 (DRAM traffic ~0.25 x the algorithmic bytes) and "
+                                 "the step is bound by the tangent-linear stencil launches' instruction issue "
+                                 "(~590 instructions per node at ~46% issue-active; the polynomial steps and "
+                                 "products take ~70% of the step)"),
                      "algorithmic_bytes_per_launch": alg,
                      "kernel": ("trapezoidal step graph (kg_* kernels under conditional WHILE nodes), one graph "
                                 "launch for the K timed steps" if a.krylov == "gmres" else
@@ -484,14 +498,14 @@ def arnoldi_probe(a):
 
 
 ADJ = dict(Nx=64, Ny=64, Nz=16, h=0.5, kappa=2.0, Bz=0.4, dt=0.1, n_steps=400, checkpoint=50, seed=5,
-           box=(24, 40, 24, 40, 0, 17))
+           box=(24, 40, 24, 40, 0, 17), s_max=1.0)
 
 
-def adjoint_workload():
+def adjoint_workload(s_max: float = ADJ["s_max"]):
     """The differentiation workload: 64x64x16 film, kappa 2, Bz 0.4, a smooth
-    seeded suppression field s(x) in [0, 0.05] (sc = 1 - s; with the
-    reference's -(1 - sc) psi / 0.1 relaxation a larger s drives psi to zero),
-    seeded psi0."""
+    seeded suppression field s(x) in [0, s_max] (sc = 1 - s; the configured
+    range is [0, 1]; with the reference's -(1 - sc) psi / 0.1 relaxation, s
+    above ~0.1 drives psi towards zero there), seeded psi0."""
     import nanowire_tdgl_b200 as tb
     w = ADJ
     p = tb.SimulationParameters(Nx=w["Nx"], Ny=w["Ny"], Nz=w["Nz"], hx=w["h"], hy=w["h"], hz=w["h"],
@@ -502,7 +516,7 @@ def adjoint_workload():
     for _ in range(6):                        # smooth: repeated 3-point averages along each axis
         for ax in range(3):
             z = (np.roll(z, 1, ax) + z + np.roll(z, -1, ax)) / 3.0
-    s_full = 0.05 * (z - z.min()) / (z.max() - z.min())
+    s_full = s_max * (z - z.min()) / (z.max() - z.min())
     sc_full = (1.0 - s_full).reshape(-1)
     def material(kappa=w["kappa"]):
         return tb.MaterialMap(kappa=np.full(p.dim_x, kappa), sc_mask=sc_full.copy(),
@@ -513,7 +527,7 @@ def adjoint_workload():
     return p, idx, material, x0
 
 
-def run_adjoint(a):
+def run_adjoint(a, s_max: float = ADJ["s_max"]):
     """Gradient of mean |psi|^2 over the centred box after 400 steps with
     respect to s(x), Bz and kappa; FP32 Krylov forward (mixed) with the FP64
     adjoint, timed; central differences (eps 1e-4) of a tight FP64 forward
@@ -521,7 +535,7 @@ def run_adjoint(a):
     import torch
     import nanowire_tdgl_b200 as tb
     w = ADJ
-    p, idx, material, x0 = adjoint_workload()
+    p, idx, material, x0 = adjoint_workload(s_max)
     t_stop = w["n_steps"] * w["dt"]
     loss = tb.box_mean_psi2(p, w["box"])
     kw = dict(material=material(), B=(0.0, 0.0, w["Bz"]), checkpoint_every=w["checkpoint"])
@@ -546,8 +560,8 @@ def run_adjoint(a):
     fd_k = (L(kappa=w["kappa"] + eps) - L(kappa=w["kappa"] - eps)) / (2 * eps)
     gs = res["grad_sc"].cpu().numpy()
     return {"form": "adjoint", "workload": "64x64x16 film (59,535 interior nodes), kappa 2, Bz 0.4, smooth s(x) in "
-                                           "[0, 0.05], loss mean |psi|^2 over the centred 16x16x16 box after 400 "
-                                           "steps dt 0.1, checkpoints every 50",
+                                           f"[0, {s_max:g}], loss mean |psi|^2 over the centred 16x16x16 box after "
+                                           "400 steps dt 0.1, checkpoints every 50",
             "seconds": el, "steps": res["steps"], "adjoint_gmres_iters": res["adjoint_iters"],
             "loss": res["loss"], "grad_Bz": float(res["grad_B"][2]), "grad_kappa": res["grad_kappa"],
             "grad_s_norm": float(np.linalg.norm(gs)),
@@ -757,13 +771,57 @@ def run_trilayer(a):
             "fp64_counters": {k: std[k] for k in ("newton_iters", "krylov_iters", "rejections", "max_krylov")}}
 
 
+def run_forms(a) -> dict:
+    """The other forms of the build, measured after the headline line of the
+    default run (one GPU), each at a reduced step count and guarded so that a
+    failure leaves the headline intact: the 256x256x64 trilayer (3 steps after
+    1 warm-up), the 64-instance batch (4 steps per instance after 1 warm-up,
+    autotuned), and the differentiation workload (400 steps forward and
+    adjoint) at s(x) in [0, 0.05] and at the configured [0, 1]."""
+    import gc
+    import torch
+    from nanowire_tdgl_b200 import engine
+    res = {}
+    def fresh():
+        engine._CACHE.clear()
+        gc.collect()
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+    def sub(**kw):
+        b = argparse.Namespace(**vars(a))
+        for k, v in kw.items():
+            setattr(b, k, v)
+        return b
+    jobs = [("trilayer", lambda: run_trilayer(sub(steps=3, warmup=1))),
+            ("batched", lambda: run_batched(sub(steps=4, warmup=1))),
+            ("adjoint", lambda: run_adjoint(a, 0.05)),
+            ("adjoint_s_0_to_1", lambda: run_adjoint(a, 1.0))]
+    for name, job in jobs:
+        fresh()
+        t0 = time.perf_counter()
+        try:
+            r = job()
+        except Exception as e:                        # keep the headline line whatever a form does
+            r = {"error": f"{type(e).__name__}: {e}"}
+        r["wall_s"] = time.perf_counter() - t0
+        res[name] = r
+    fresh()
+    deg = res.get("adjoint_s_0_to_1", {})
+    if "loss" in deg:
+        deg["note"] = ("with s(x) up to 1 the reference's relaxation -(1 - sc) psi / 0.1 (sc = 1 - s) drives psi "
+                       "to ~0 wherever s exceeds ~0.1, so the box loss is ~0 and its finite differences are "
+                       "round-off; the gradient check is the [0, 0.05] run")
+    return res
+
+
 def main():
     a = parse()
+    os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")   # before CUDA starts: one queue per batch stream
     if a.form == "trilayer":
         print(json.dumps(run_trilayer(a)), flush=True)
         return 0
     if a.form == "adjoint":
-        print(json.dumps(run_adjoint(a)), flush=True)
+        print(json.dumps(run_adjoint(a, a.adj_smax)), flush=True)
         return 0
     if a.form == "batched":
         os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")   # before CUDA is initialised
@@ -816,6 +874,8 @@ def main():
                 out["vs_oracle_note"] = (f"state after step 1 from the seeded state: this run's {a.precision} "
                                          "stepper against the oracle's FP64 finite-difference GCR step (same "
                                          "tolerances); max_abs over all state entries")
+        if world == 1 and not a.no_forms:
+            out["forms"] = run_forms(a)
         print(json.dumps(out), flush=True)
     return 0
 
