@@ -127,18 +127,17 @@ def algorithmic_bytes(n_int: int, precision: str, st: dict, poly_deg: int = 0) -
     (orthogonalisation j + 2 vectors, product 3, projections j + 2) plus the
     last step's orthogonalisation (its products are skipped once its stop
     check has ended the solve), within a few percent of the model at m ~ 25.
-    With the polynomial preconditioner of degree d, every Arnoldi column and
-    every Newton correction takes d more stencil launches (counted in
-    jvp_evals, 3 SK + F each) that also read the vector they precondition
-    (+SK each), and the correction is first combined from the basis
-    (m + 1 vectors per Newton iteration).
+    With the polynomial preconditioner of degree d, every Arnoldi column takes
+    d more stencil launches (counted in jvp_evals, 3 SK + F each) that also
+    read the vector they precondition (+SK each); the last of them keeps
+    p(A) U_j as the preconditioned basis vector the Newton correction combines
+    (in place of the basis vector itself, so the update's traffic is
+    unchanged).
     """
     S64 = 40.0 * n_int
     SK = (20.0 if precision == "mixed" else 40.0) * n_int
     F = 1.0 * n_int
-    poly = poly_deg * (st["krylov_iters"] + st["newton_iters"]) * SK
-    if poly_deg:
-        poly += (st["krylov_iters"] + st["newton_iters"]) * SK
+    poly = poly_deg * st["krylov_iters"] * SK
     return (st["rhs_evals"] * (2 * S64 + F) + st["jvp_evals"] * (3 * SK + F)
             + (st["krylov_sq"] + 7 * st["krylov_iters"]) * SK + 7 * S64 * st["newton_iters"] + poly)
 
@@ -149,11 +148,10 @@ def graph_launches(st: dict, jvp: str, poly_deg: int = 0) -> int:
     (orthogonalisation, stop check, product, projections; analytic products;
     the last step's product and projections return at once) or 5 m
     (finite-difference products); with the polynomial preconditioner of
-    degree d, d more per Arnoldi step and d + 1 more per Newton iteration."""
+    degree d, d more per Arnoldi step."""
     base = 7 * (st["steps"] + st["rejections"]) + 4 * st["newton_iters"]
     if jvp == "analytic":
-        return (base + (4 + poly_deg) * (st["krylov_iters"] + st["newton_iters"])
-                + (poly_deg + 1 if poly_deg else 0) * st["newton_iters"])
+        return base + (4 + poly_deg) * (st["krylov_iters"] + st["newton_iters"])
     return base + 5 * st["krylov_iters"]
 
 

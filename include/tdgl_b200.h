@@ -299,8 +299,12 @@ int tdgl_euler_run(tdgl_ctx* ctx, double* x_dev, double* t, double t_stop, doubl
  * process exits).  Limits: 32768 interior nodes, 262144 full-grid nodes,
  * 65536 entries per hole list; larger inputs return TDGL_EINVAL before any
  * device work.  Calls share that array: calls that overlap on the GPU race.
- * The first call on a device looks the array up (cudaGetSymbolAddress); make
- * it before any stream capture.  No counterpart in the reference. */
+ * The first call on a device looks the array up (cudaGetSymbolAddress) and
+ * keeps its address for the life of the process: make it before any stream
+ * capture, and do not call again after cudaDeviceReset.  The material
+ * descriptor's arrays are host memory copied on every call; a call that has
+ * any returns TDGL_EINVAL while its stream is capturing.  No counterpart in
+ * the reference. */
 int tdgl_eval_f_noalloc(const tdgl_grid_desc* grid, const tdgl_material_desc* material, const double* x_ref,
                         double* f_ref, double Bx, double By, double Bz, tdgl_stream_t stream);
 

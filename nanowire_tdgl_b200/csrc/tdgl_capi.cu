@@ -146,7 +146,7 @@ struct tdgl_ctx {
   int poly_req = -1, poly_deg = 0;
   double k2max = 0.0;
   void* PW[2] = {nullptr, nullptr};
-  void* PC = nullptr;
+  void* PB = nullptr;     // preconditioned basis p(A) U_j ((kmax + 1) vectors)
   // queued step-graph launches (tdgl_trap_launch / tdgl_trap_launch_next):
   // per launch slot a pinned input and output control block and a completion
   // event; up to two launches queued, collected in order
@@ -747,7 +747,7 @@ static GArgs<T> make_gargs(tdgl_ctx* c) {
   A.poly_rho = poly_rho_bound(c);
   A.PW[0] = (T*)c->PW[0];
   A.PW[1] = (T*)c->PW[1];
-  A.PC = (T*)c->PC;
+  A.PB = (T*)c->PB;
   return A;
 }
 
@@ -837,9 +837,9 @@ static int setup_tl(tdgl_ctx* c) {
   const cuuint32_t box[5] = {(cuuint32_t)(32 * tnx + 4), (cuuint32_t)kTlBoxY, 1u, (cuuint32_t)kTlComp, 1u};
   const cuuint32_t es[5] = {1u, 1u, 1u, 1u, 1u};
   if (g.ncomp != kTlComp || g.mj % 4 || c->npf % 4) return fail(TDGL_ECUDA, "full-grid layout not TMA-aligned");
-  void* base[5] = {c->XLe, c->UB, c->PW[0], c->PW[1], c->PC};
+  void* base[5] = {c->XLe, c->UB, c->PW[0], c->PW[1], c->PB};
   for (int t = 0; t < 5; ++t) {
-    const cuuint32_t rank = t == TM_UB ? 5u : 4u;
+    const cuuint32_t rank = (t == TM_UB || t == TM_PB) ? 5u : 4u;
     CUresult r = encode(&c->tlm.m[t], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, rank, base[t], dims, strides, box, es,
                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
@@ -873,7 +873,7 @@ static int ensure_arnoldi_ws(tdgl_ctx* c) {
   if ((rc = ctx_alloc(c, &c->Zb[1], vb))) return rc;
   if ((rc = ctx_alloc(c, &c->PW[0], vb))) return rc;
   if ((rc = ctx_alloc(c, &c->PW[1], vb))) return rc;
-  if ((rc = ctx_alloc(c, &c->PC, vb))) return rc;
+  if ((rc = ctx_alloc(c, &c->PB, vb * (c->kmax + 1)))) return rc;
   c->poly_deg = poly_setting(c);
   const size_t nparts = std::max((size_t)c->num_sms * kMaxBlocksPerSm, (size_t)c->ntiles);
   if ((rc = ctx_alloc(c, (void**)&c->part_arn, sizeof(double) * (c->kmax + 2) * nparts))) return rc;

@@ -150,14 +150,15 @@ struct GArgs {
   unsigned* gticket;   // [ngroups] arrival counters
   // polynomial right preconditioner of the analytic-product solves: degree
   // (0: none), an upper bound of the spectral radius of J, the Horner buffers
-  // (ping-pong) and the Newton correction before the polynomial; pstep / pmode
-  // are per kernel node (Horner step; 0: Krylov direction U_ja, 1: correction)
+  // (ping-pong), and the preconditioned basis PB_j = p(A) U_j ((kmax + 1)
+  // vectors like UB), written by the last Horner step of Arnoldi step j and
+  // read by its product; the Newton correction is sum_i c_i PB_i.  pstep is
+  // per kernel node (the Horner step).
   int poly_deg;
   double poly_rho;
   T* PW[2];
-  T* PC;
-  int pstep, pmode;
-  int upd_single;      // kg_update_fused adds PW[0] (the preconditioned correction) alone
+  T* PB;
+  int pstep;
 };
 
 template <typename T> __host__ __device__ __forceinline__ double* kry_sj(const GArgs<T>& A) { return A.kry; }
@@ -718,12 +719,11 @@ __global__ void __launch_bounds__(kThreads, 3) kg_update_fused(GArgs<T> A) {
   kt_begin(A.dev, KT_UPDATE);
   constexpr int NC = D3 ? 5 : 4;
   const Grid& g = A.g;
-  // with the polynomial preconditioner the correction p(A) sum_i c_i U_i is
-  // already formed in PW[0]: one vector with coefficient 1
-  const double one[4] = {1.0, 0.0, 0.0, 0.0};
-  const int nk = A.upd_single ? 1 : d->j;
-  const double* cj = A.upd_single ? one : kry_cj(A);
-  const T* UBase = A.upd_single ? A.PW[0] : A.UB;
+  // with the polynomial preconditioner the correction is p(A) sum_i c_i U_i
+  // = sum_i c_i PB_i (PB_i = p(A) U_i, kept by the Arnoldi steps)
+  const int nk = d->j;
+  const double* cj = kry_cj(A);
+  const T* UBase = A.poly_deg > 0 ? A.PB : A.UB;
   const double czxy = d->czxy, cyzx = d->cyzx, cxyz = d->cxyz;
   double acc[1] = {0.0};
   // basis on the full grid: one node per thread
@@ -1016,7 +1016,7 @@ __global__ void __launch_bounds__(kThreads, 3) kg_arn_apply(GArgs<T> A) {
   const int ja = d->ja;
   const long npf = A.npf;
   // product input: U_ja, or p(A) U_ja from the polynomial steps
-  const T* Uj = A.poly_deg > 0 ? A.PW[0] : A.UB + (long)ja * A.vs;
+  const T* Uj = (A.poly_deg > 0 ? A.PB : A.UB) + (long)ja * A.vs;
   T* Zout = A.Zb[ja & 1];
   const double dth = d->dta / 2.0;
   const int i = 1 + blockIdx.x * 32 + (threadIdx.x & 31), j = 1 + blockIdx.y * 8 + (threadIdx.x >> 5);
@@ -1099,24 +1099,24 @@ __device__ void poly_setup(const GArgs<T>& A, GDev* d) {
 
 // One Horner step of the preconditioner on the full grid:
 //   W_k = e_k V + beta t(W_in),  t(W) = (A W - theta W) / delta,
-// V = U_ja (Krylov direction, pmode 0) or the Newton correction PC (pmode 1);
-// the first step (k = d - 1) starts from W_in = V with beta = e_d, the others
-// read W_{k+1} with beta = 1.  The stencil is the product kernel's (dead
-// links from the per-node mask); W_k is written with its face values.
+// V = U_ja, the Krylov direction; the first step (k = d - 1) starts from
+// W_in = V with beta = e_d, the others read W_{k+1} with beta = 1, and the
+// last (k = 0) writes p(A) U_ja into the preconditioned basis PB_ja.  The
+// stencil is the product kernel's (dead links from the per-node mask); W_k
+// is written with its face values.
 template <typename T, bool D3>
 __global__ void __launch_bounds__(kThreads, 3) kg_arn_poly(GArgs<T> A) {
   GDev* d = A.dev;
   if (!gdev_ok(d)) return;
-  if (A.pmode && d->newton_failed) return;
-  if (!A.pmode && d->arn_stop && !A.standalone) return;   // the solve stopped at this step's check
+  if (d->arn_stop && !A.standalone) return;   // the solve stopped at this step's check
   kt_begin(d, KT_ARN_APPLY);
   constexpr int NC = D3 ? 5 : 4;
   const Grid& g = A.g;
   const long npf = A.npf;
   const int kst = A.pstep, deg = A.poly_deg;
-  const T* V = A.pmode ? A.PC : A.UB + (long)d->ja * A.vs;
+  const T* V = A.UB + (long)d->ja * A.vs;
   const T* Win = kst == deg - 1 ? V : A.PW[(kst + 1) & 1];
-  T* Wout = A.PW[kst & 1];
+  T* Wout = kst == 0 ? A.PB + (long)d->ja * A.vs : A.PW[kst & 1];
   const double alpha = d->poly_e[kst], beta = kst == deg - 1 ? d->poly_e[deg] : 1.0;
   const double th = d->poly_theta, ide = 1.0 / d->poly_delta, dth = d->dta / 2.0;
   const int i = 1 + blockIdx.x * 32 + (threadIdx.x & 31), j = 1 + blockIdx.y * 8 + (threadIdx.x >> 5);
@@ -1148,29 +1148,6 @@ __global__ void __launch_bounds__(kThreads, 3) kg_arn_poly(GArgs<T> A) {
     write_eff<T, D3, true>(g, Wout, npf, i, j, k, z, 0.0, 0.0, 0.0);
   }
   kt_end(d, KT_ARN_APPLY);
-}
-
-// Newton correction before the preconditioner: PC = sum_i c_i U_i over every
-// entry of the full-grid vectors (the combination of face values is the face
-// value of the combination); the polynomial steps then form p(A) PC.
-template <typename T>
-__global__ void __launch_bounds__(kThreads) kg_poly_combine(GArgs<T> A) {
-  GDev* d = A.dev;
-  if (!gdev_ok(d) || d->newton_failed) return;
-  if (blockIdx.x == 0 && threadIdx.x == 0) d->jvp_evals += A.poly_deg;
-  const int nk = d->j;
-  const double* cj = kry_cj(A);
-  const long vs = A.vs, nq = vs / 4;
-  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < nq; q += (long)gridDim.x * blockDim.x) {
-    const long e = 4 * q;
-    double v[4] = {0.0, 0.0, 0.0, 0.0};
-    for (int i = 0; i < nk; ++i) {
-      const V4<T> a = ld4(A.UB + (long)i * vs + e);
-      const double c = cj[i];
-      v[0] += c * (double)a.a; v[1] += c * (double)a.b; v[2] += c * (double)a.c; v[3] += c * (double)a.d;
-    }
-    st4(A.PC + e, v);
-  }
 }
 
 // Blocks of a two-level fold: groups of kTileGroup consecutive blocks.
@@ -1367,7 +1344,7 @@ __global__ void __launch_bounds__(kThreads, 3) kg_arn_apply_dots(GArgs<T> A) {
   const int ja = d->ja;
   const long npf = A.npf;
   // product input: U_ja, or p(A) U_ja from the polynomial steps
-  const T* Uj = A.poly_deg > 0 ? A.PW[0] : A.UB + (long)ja * A.vs;
+  const T* Uj = (A.poly_deg > 0 ? A.PB : A.UB) + (long)ja * A.vs;
   T* Zout = A.Zb[ja & 1];
   const double dth = d->dta / 2.0;
   const int i = 1 + blockIdx.x * 32 + (threadIdx.x & 31), j = 1 + blockIdx.y * 8 + (threadIdx.x >> 5);

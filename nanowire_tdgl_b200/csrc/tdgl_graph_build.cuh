@@ -115,19 +115,7 @@ cudaError_t build_trap_graph(GArgs<T> A, const TlMaps* tm, int chunks, cudaGraph
   TDGL_GCK(cn.loop(A.h_krylov, &krylov_body));
   TDGL_GCK(cn.kernel((const void*)kg_newton_solve<T>, 1, kThreads, 0, A));
   const dim3 tiles(A.arn_gx, A.arn_gy, D3 ? A.g.nz : 1);
-  if (A.fused && A.poly_deg > 0) {
-    // Newton correction p(A) sum_i c_i U_i, then the update with that one vector
-    TDGL_GCK(cn.kernel((const void*)kg_poly_combine<T>, nb, kThreads, 0, A));
-    for (int k = A.poly_deg - 1; k >= 0; --k) {
-      GArgs<T> P = A;
-      P.pstep = k;
-      P.pmode = 1;
-      TDGL_GCK((add_tl<T, D3>(cn, P, tm, chunks, true)));
-    }
-    GArgs<T> U = A;
-    U.upd_single = 1;
-    TDGL_GCK(cn.kernel((const void*)kg_update_fused<T, D3>, nb, kThreads, 0, U));
-  } else if (A.fused) {
+  if (A.fused) {                    // x += sum_i c_i U_i, or sum_i c_i p(A) U_i with the preconditioner
     TDGL_GCK(cn.kernel((const void*)kg_update_fused<T, D3>, nb, kThreads, 0, A));
   } else {
     TDGL_GCK(cn.kernel((const void*)kg_update<T, D3>, nb, kThreads, 0, A));
@@ -142,10 +130,9 @@ cudaError_t build_trap_graph(GArgs<T> A, const TlMaps* tm, int chunks, cudaGraph
     TDGL_GCK(cudaFuncSetAttribute((const void*)kg_arn_dots<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smd));
     TDGL_GCK(ck.kernel((const void*)kg_arn_orth<T>, A.nblk_orth, kThreads, smo, A));
     TDGL_GCK(ck.kernel((const void*)kg_arn_check<T>, 1, kThreads, 0, A));
-    for (int k = A.poly_deg - 1; k >= 0; --k) {   // p(A) U_ja into PW[0]
+    for (int k = A.poly_deg - 1; k >= 0; --k) {   // p(A) U_ja into PB_ja
       GArgs<T> P = A;
       P.pstep = k;
-      P.pmode = 0;
       TDGL_GCK((add_tl<T, D3>(ck, P, tm, chunks, true)));
     }
     if (A.apply_dots) {

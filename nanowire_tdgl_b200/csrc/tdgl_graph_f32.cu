@@ -66,7 +66,6 @@ cudaError_t arnoldi_probe_f32(const GArgs<float>& A, const TlMaps* tm, int chunk
     for (int k = (kernels & 16) ? A.poly_deg - 1 : -1; k >= 0 && e == cudaSuccess; --k) {
       GArgs<float> P = A;
       P.pstep = k;
-      P.pmode = 0;
       e = launch_tl(P, tm, chunks, true, s);
     }
     if ((kernels & 2) && e == cudaSuccess) e = launch_tl(A, tm, chunks, false, s);

@@ -42,7 +42,6 @@ cudaError_t arnoldi_probe_f64(const GArgs<double>& A, int launches, int kernels,
     for (int k = (kernels & 16) ? A.poly_deg - 1 : -1; k >= 0; --k) {
       GArgs<double> P = A;
       P.pstep = k;
-      P.pmode = 0;
       if (A.g.is3d) kg_arn_poly<double, true><<<grid, kThreads, 0, s>>>(P);
       else kg_arn_poly<double, false><<<grid, kThreads, 0, s>>>(P);
     }

@@ -17,7 +17,11 @@
 // overwrites what it uses, so calls that overlap on the GPU (different
 // streams, or different host threads) race and must be serialised by the
 // caller.  The first call on a device looks up the array's device address
-// (cudaGetSymbolAddress); make that first call before any stream capture.
+// (cudaGetSymbolAddress) and keeps it for the life of the process; make that
+// first call before any stream capture, and do not call the entry point again
+// after cudaDeviceReset (the kept address would be stale).  The material
+// descriptor's arrays are host memory copied on every call, so a call that
+// has any is refused while its stream is capturing.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -182,7 +186,7 @@ extern "C" int tdgl_eval_f_noalloc(const tdgl_grid_desc* gd, const tdgl_material
   if (dimx > kMaxFull)
     return err(TDGL_EINVAL, "tdgl_eval_f_noalloc handles at most " + std::to_string(kMaxFull) +
                                 " full-grid nodes; this grid has " + std::to_string(dimx));
-  for (int a = 0; a < 3; ++a) {
+  for (int a = 0; a < (d3 ? 3 : 2); ++a) {      // the axes build_geometry reads (z only in 3-D)
     if (!md) break;
     if (md->n_hole_links[a] > kMaxLinks || md->n_hole_interior[a] > kMaxLinks)
       return err(TDGL_EINVAL, "tdgl_eval_f_noalloc takes at most " + std::to_string(kMaxLinks) +
@@ -192,6 +196,17 @@ extern "C" int tdgl_eval_f_noalloc(const tdgl_grid_desc* gd, const tdgl_material
     for (int64_t t = 0; t < md->n_hole_interior[a]; ++t)
       if (md->hole_interior[a][t] < 0 || md->hole_interior[a][t] >= n)
         return err(TDGL_EINVAL, "hole interior index out of range");
+  }
+  bool host_arrays = md && (md->kappa_full || md->sc_interior);
+  for (int a = 0; md && a < (d3 ? 3 : 2); ++a)
+    host_arrays = host_arrays || md->n_hole_links[a] > 0 || md->n_hole_interior[a] > 0;
+  if (host_arrays) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaError_t ce = cudaStreamIsCapturing(stream, &cs);
+    if (ce != cudaSuccess) return err(TDGL_ECUDA, std::string("cudaStreamIsCapturing: ") + cudaGetErrorString(ce));
+    if (cs != cudaStreamCaptureStatusNone)
+      return err(TDGL_EINVAL, "tdgl_eval_f_noalloc copies the material descriptor's host arrays on every call; "
+                              "such a call cannot be made while the stream is capturing");
   }
   unsigned char* base = nullptr;
   int rc = scratch_address(&base);

@@ -64,10 +64,10 @@ struct TlShape {
   static_assert((kSlotF * 4) % 128 == 0 && kRing <= 256 && (kBoxX * 4) % 16 == 0, "staged box shape");
 };
 
-// Tensor maps of the staged vectors: 0 linearisation copy, 1 the basis (5-D:
-// the fifth coordinate is the basis vector), 2 and 3 the Horner buffers, 4 the
-// Newton correction.
-enum TlMap : int { TM_X = 0, TM_UB = 1, TM_PW0 = 2, TM_PW1 = 3, TM_PC = 4 };
+// Tensor maps of the staged vectors: 0 linearisation copy, 1 the basis, 2 and
+// 3 the Horner buffers, 4 the preconditioned basis (the bases are 5-D: the
+// fifth coordinate is the basis vector).
+enum TlMap : int { TM_X = 0, TM_UB = 1, TM_PW0 = 2, TM_PW1 = 3, TM_PB = 4 };
 struct alignas(64) TlMaps {
   CUtensorMap m[5];
   int nx;        // nodes per thread along x of the kernel the maps' boxes are shaped for (1 or 2)
@@ -234,11 +234,7 @@ __global__ void __launch_bounds__(kThreads, TlShape<NX>::kMinBlocks)
   __shared__ __align__(8) uint64_t bar[SL];
   GDev* d = A.dev;
   if (!gdev_ok(d)) return;
-  if (POLY && A.pmode) {
-    if (d->newton_failed) return;
-  } else if (d->arn_stop && !A.standalone) {
-    return;                                         // the solve stopped at this step's check
-  }
+  if (d->arn_stop && !A.standalone) return;       // the solve stopped at this step's check
   kt_begin(d, KT_ARN_APPLY);
   const Grid& g = A.g;
   const long npf = A.npf;
@@ -255,12 +251,12 @@ __global__ void __launch_bounds__(kThreads, TlShape<NX>::kMinBlocks)
       const int kst = A.pstep, deg = A.poly_deg;
       const bool first = kst == deg - 1;           // W_in is V itself
       if (first) {
-        pm = A.pmode ? TM_PC : TM_UB;
+        pm = TM_UB;
       } else {
         pm = ((kst + 1) & 1) ? TM_PW1 : TM_PW0;
-        Vg = A.pmode ? A.PC : A.UB + (long)ja * A.vs;
+        Vg = A.UB + (long)ja * A.vs;
       }
-      out = A.PW[kst & 1];
+      out = kst == 0 ? A.PB + (long)ja * A.vs : A.PW[kst & 1];   // the last step: PB_ja = p(A) U_ja
       const double beta = first ? d->poly_e[deg] : 1.0, ide = 1.0 / d->poly_delta;
       const double e = d->poly_e[kst];
       // z = e V + beta ((W - dth J W) - theta W) / delta
@@ -268,7 +264,7 @@ __global__ void __launch_bounds__(kThreads, TlShape<NX>::kMinBlocks)
       cv = first ? 0.0f : (float)e;
       cr = (float)(-beta * dth * ide);
     } else {
-      if (A.poly_deg > 0) pm = TM_PW0;
+      if (A.poly_deg > 0) pm = TM_PB;
       out = A.Zb[ja & 1];
       cr = (float)(-dth);                           // z = W - dth J W
     }
@@ -282,7 +278,7 @@ __global__ void __launch_bounds__(kThreads, TlShape<NX>::kMinBlocks)
   const int bx = blockIdx.x * S::kTx, by = blockIdx.y * kTlTy;   // box origin: (i0 - 1, j0 - 1)
   const CUtensorMap* mx = &M.m[TM_X];
   const CUtensorMap* mp = &M.m[pm];
-  const bool p5 = pm == TM_UB;
+  const bool p5 = pm == TM_UB || pm == TM_PB;
   int issued = 0;                                  // thread 0: staged planes issued so far
   auto issue = [&](int q) {                        // staged plane q into slot q % SL
     const int s = q % SL;

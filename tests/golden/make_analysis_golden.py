@@ -4,7 +4,7 @@ reference (src/tdgl3d/analysis/vortex_counting.py, convergence.py).
 Run where the reference source tree is available (imported read-only from
 ``<reference>/src``)::
 
-    python tests/golden/make_analysis_golden.py --reference /root/reference
+    python tests/golden/make_analysis_golden.py --reference <path to the tdgl3d checkout>
 
 Writes ``analysis.npz`` next to this script: seeded states with phase
 windings (2-D and a 3-D film with a hole), the reference's plaquette vortex
@@ -49,8 +49,11 @@ def vortex_state(params, centers, sc=None, rng=None, phi_scale=0.0):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default=os.environ.get("TDGL3D_REFERENCE", "/root/reference"))
+    ap.add_argument("--reference", default=os.environ.get("TDGL3D_REFERENCE"),
+                    help="checkout of omedeiro/nanowire_tdgl (its src/ is imported); or set TDGL3D_REFERENCE")
     a = ap.parse_args()
+    if not a.reference:
+        ap.error("--reference (or TDGL3D_REFERENCE) is required")
     sys.path.insert(0, os.path.join(a.reference, "src"))
     import tdgl3d
     from tdgl3d.analysis.convergence import check_steady_state, compute_convergence_metrics

@@ -3,7 +3,7 @@
 Run in a container where the reference source tree is mounted (it is imported
 read-only from ``<reference>/src``)::
 
-    python tests/golden/make_golden.py --reference /root/reference
+    python tests/golden/make_golden.py --reference <path to the tdgl3d checkout>
 
 It writes small ``.npz`` files next to this script.  The fixtures pin the CPU
 oracle (``oracle/tdgl_oracle.py``) and the device path to the reference's own
@@ -141,9 +141,12 @@ def case_meta(case):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("TDGL3D_REFERENCE"),
+                    help="checkout of omedeiro/nanowire_tdgl (its src/ is imported); or set TDGL3D_REFERENCE")
     ap.add_argument("--skip-long", action="store_true", help="skip the 101-step trajectory")
     args = ap.parse_args()
+    if not args.reference:
+        ap.error("--reference (or TDGL3D_REFERENCE) is required")
     sys.path.insert(0, os.path.join(args.reference, "src"))
     import tdgl3d as td
     from tdgl3d.physics.rhs import BoundaryVectors, eval_f

@@ -49,6 +49,50 @@ def test_noalloc_matches_context_eval_f(name):
         assert _rel(f, want) < RTOL
 
 
+def _limit_device():
+    """33x33x33 cells: 32,768 interior nodes (the entry point's limit), a hole
+    through part of the thickness, per-node kappa and fractional sc."""
+    import nanowire_tdgl_b200 as tb
+    p = tb.SimulationParameters(Nx=33, Ny=33, Nz=33, hx=0.5, hy=0.5, hz=0.5, kappa=2.0)
+    dev = tb.Device(p, applied_field=tb.AppliedField(Bx=0.1, Bz=0.5, t_on_fraction=1.0))
+    dev.add_hole([(4.0, 4.0), (8.0, 4.0), (8.0, 7.5), (4.0, 7.5)], z_range=(3, 20))
+    m = dev.material
+    rng = np.random.default_rng(21)
+    kappa = m.kappa * (1.0 + 0.3 * rng.random(m.kappa.shape))
+    sc = m.interior_sc_mask * (0.5 + 0.5 * rng.random(m.interior_sc_mask.shape))
+    dev._material = tb.MaterialMap(kappa=kappa, sc_mask=m.sc_mask.copy(), interior_sc_mask=sc)
+    assert p.n_interior == 32768
+    return dev
+
+
+def test_noalloc_at_its_limit_after_a_smaller_grid():
+    """At the maximum size, after a smaller geometry has filled the array:
+    two calls in a row (different states) against tdgl_eval_f."""
+    from nanowire_tdgl_b200 import _lib
+    from nanowire_tdgl_b200.engine import descriptors, grid_for, stream_handle
+    lib = _lib.load()
+    small = device_from_fixture(golden("case_3d_hole"))
+    big = _limit_device()
+    rng = np.random.default_rng(22)
+    for dev, calls in ((small, 1), (big, 2)):
+        ctx_grid = grid_for(dev.params, dev.idx, dev.material)
+        gd, md, keep = descriptors(dev.params, dev.idx, dev.material)
+        n = dev.params.n_interior
+        for _ in range(calls):
+            X = np.zeros(dev.params.n_state, dtype=np.complex128)
+            X[:n] = 1.0 + 0.3 * (rng.standard_normal(n) + 1j * rng.standard_normal(n))
+            X[n:] = 0.2 * rng.standard_normal(dev.params.n_state - n)
+            B = (0.1, 0.0, 0.5)
+            want = ctx_grid.eval_f_ref(X, B)
+            x = ctx_grid.ref_tensor(X)
+            f = torch.full_like(x, float("nan"))
+            rc = lib.tdgl_eval_f_noalloc(C.byref(gd), C.byref(md), C.c_void_p(x.data_ptr()),
+                                         C.c_void_p(f.data_ptr()), *B, stream_handle())
+            assert rc == _lib.TDGL_OK, lib.tdgl_last_error()
+            torch.cuda.synchronize()
+            assert _rel(f, want) < RTOL
+
+
 def test_noalloc_rejects_grids_beyond_its_limit():
     from nanowire_tdgl_b200 import _lib
     lib = _lib.load()
