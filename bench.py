@@ -46,10 +46,10 @@ WORKLOAD_N_INTERIOR = 127 * 127 * 31
 # workload at the default preconditioner degree (5), from a graph-level ncu
 # capture (dram__bytes_read.sum + dram__bytes_write.sum) of the timed 2-step
 # launch of `bench.py --steps 2 --warmup 3 --no-fp64 --no-e2e
-# --no-cpu-baseline --no-forms`: 1.299 GB read + 1.992 GB written = 3.291 GB
-# against 13.317 GB algorithmic.  The preconditioned solves keep their basis
-# (<= 7 vectors of 11 MB) and the stencil vectors in L2.
-DRAM_PER_ALG_BYTE = 0.2471
+# --no-cpu-baseline --no-forms`: 1.055 GB read + 1.342 GB written = 2.397 GB
+# against 11.954 GB algorithmic.  The preconditioned solves keep their bases
+# (<= 7 vectors of 11 MB each) and the stencil vectors in L2.
+DRAM_PER_ALG_BYTE = 0.2005
 DRAM_RATIO_DEGREE = 5
 
 
