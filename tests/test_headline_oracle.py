@@ -84,3 +84,23 @@ def test_one_step_at_headline_size(headline, precision, krylov):
     rel = _psi2_rel(x1, h["x1"], p.n_interior)
     assert err < 1e-7, f"{precision}/{krylov}: max |x - oracle| = {err:.3e}"
     assert rel < 1e-6, f"{precision}/{krylov}: |psi|^2 relative L2 = {rel:.3e}"
+
+
+def test_eval_f_at_trilayer_size():
+    """The 256x256x64 S/I/S trilayer with its 64x64 hole (4,096,575 interior
+    nodes; the large configuration of the bench's forms): FP64 RHS against
+    the oracle at 1e-12 relative, with links away from zero."""
+    import bench
+    from nanowire_tdgl_b200.engine import grid_for
+    from oracle import tdgl_oracle as orc
+    dev, x0 = bench.trilayer_device()
+    og = orc.make_grid(dev.params, dev.idx, dev.material)
+    g = grid_for(dev.params, dev.idx, dev.material)
+    n = dev.params.n_interior
+    X = x0.copy()
+    X[n:] = 0.3 * np.random.default_rng(13).standard_normal(X.size - n) + 0j
+    B = (0.0, 0.0, bench.TRI["Bz"])
+    F = g.eval_f_ref(X, B).cpu().numpy()
+    want = orc.eval_f(X, og, *B)
+    rel = np.max(np.abs(F - want)) / np.max(np.abs(want))
+    assert rel < 1e-12, f"relative max error {rel:.3e}"
