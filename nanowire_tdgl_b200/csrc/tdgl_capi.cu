@@ -160,6 +160,7 @@ struct tdgl_ctx {
   uint8_t* imask = nullptr;
   uint32_t* deadmask = nullptr;   // per interior node: dead links read by the Arnoldi product
   uint8_t* ldead = nullptr;       // per full-grid node: its dead links (TMA-staged stencil)
+  TlSched* tls = nullptr;         // the TMA-staged stencil's two sets of work-item claim counters
   // TMA-staged tangent-linear stencil (FP32 vectors, 3-D grids): tensor maps of
   // the staged vectors and the z-chunks per tile column
   TlMaps tlm{};
@@ -735,6 +736,8 @@ static GArgs<T> make_gargs(tdgl_ctx* c) {
   A.apply_dots = c->apply_dots;
   A.deadmask = c->deadmask;
   A.ldead = c->ldead;
+  A.tls = c->tl_on ? c->tls : nullptr;
+  A.tl_par = 0;
   A.ntiles = c->ntiles;
   A.ngroups = c->ngroups;
   A.gpart = c->gpart;
@@ -808,7 +811,9 @@ static int apply_dots_setting(const tdgl_ctx* c) {
 // dimensions (x, y, z, component[, vector]) with the padded row pitch, boxes
 // of (32 NX + 4) x 10 x 1 x 5 entries for the kernel with NX nodes per thread
 // (TDGL_TL_NX, default 2).  z-chunks per tile column: TDGL_TL_CHUNKS, else as
-// many as keep every block of the launch resident at once.
+// many as keep every block of the launch resident at once.  The stencil nodes
+// of the step graph depend programmatically on the node before them unless
+// TDGL_PDL=0.
 static int setup_tl(tdgl_ctx* c) {
   c->tl_on = false;
   const Grid& g = c->g;
@@ -834,6 +839,18 @@ static int setup_tl(tdgl_ctx* c) {
   if (const char* e = std::getenv("TDGL_TL_NX"))
     if (std::atoi(e) == 1 || std::atoi(e) == 2) tnx = std::atoi(e);
   c->tlm.nx = tnx;
+  // programmatic dependent launches of the stencil nodes: TDGL_PDL=0 turns them off
+  c->tlm.pdl = 1;
+  // pair coefficients of the two-nodes-per-thread kernel (uniform kappa; the
+  // 1 / h^2 entries serve a per-node kappa too)
+  tl_pair_coef(c->tlm.k2, make_float2((float)(g.kappa2 / g.hx2), (float)(g.kappa2 / g.hx2)),
+               make_float2((float)(g.kappa2 / g.hy2), (float)(g.kappa2 / g.hy2)),
+               make_float2((float)(g.kappa2 / g.hz2), (float)(g.kappa2 / g.hz2)));
+  c->tlm.k2[K_IHX] = make_float2((float)g.ihx2, (float)g.ihx2);
+  c->tlm.k2[K_IHY] = make_float2((float)g.ihy2, (float)g.ihy2);
+  c->tlm.k2[K_IHZ] = make_float2((float)g.ihz2, (float)g.ihz2);
+  if (const char* e = std::getenv("TDGL_PDL"))
+    if (e[0] == '0') c->tlm.pdl = 0;
   const cuuint32_t box[5] = {(cuuint32_t)(32 * tnx + 4), (cuuint32_t)kTlBoxY, 1u, (cuuint32_t)kTlComp, 1u};
   const cuuint32_t es[5] = {1u, 1u, 1u, 1u, 1u};
   if (g.ncomp != kTlComp || g.mj % 4 || c->npf % 4) return fail(TDGL_ECUDA, "full-grid layout not TMA-aligned");
@@ -851,6 +868,10 @@ static int setup_tl(tdgl_ctx* c) {
   if (const char* e = std::getenv("TDGL_TL_CHUNKS"))
     if (std::atoi(e) > 0) ch = std::atoi(e);
   c->tl_chunks = std::min(std::max(ch, 1), g.nz);
+  if (!c->tls) {
+    int rc = ctx_alloc(c, (void**)&c->tls, 2 * sizeof(TlSched));   // zeroed
+    if (rc) return rc;
+  }
   c->tl_on = true;
   return TDGL_OK;
 }

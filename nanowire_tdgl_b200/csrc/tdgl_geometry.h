@@ -134,6 +134,24 @@ inline int build_geometry(const tdgl_grid_desc* gd, const tdgl_material_desc* md
         }
         if (slow) nf[dev_of(i, j, k)] |= NF_SLOW;
       }
+  // face copies (the ghost node across each face that a face node writes):
+  // NF_GHOSTLF where such a ghost carries hole links, so that the copies read
+  // the link flags only at those nodes
+  if (any_hole) {
+    for (long k = (d3 ? 1 : 0); k <= (d3 ? Nz - 1 : 0); ++k)
+      for (long j = 1; j <= Ny - 1; ++j)
+        for (long i = 1; i <= Nx - 1; ++i) {
+          bool h = false;
+          auto ghost = [&](long gi, long gj, long gk) { h = h || lf[gi + mj * gj + mk * gk] != 0; };
+          if (i == 1) ghost(g.px ? Nx : 0, j, k);
+          if (i == Nx - 1) ghost(g.px ? 0 : Nx, j, k);
+          if (j == 1) ghost(i, g.py ? Ny : 0, k);
+          if (j == Ny - 1) ghost(i, g.py ? 0 : Ny, k);
+          if (d3 && k == 1) ghost(i, j, g.pz ? Nz : 0);
+          if (d3 && k == Nz - 1) ghost(i, j, g.pz ? 0 : Nz);
+          if (h) nf[dev_of(i, j, k)] |= NF_GHOSTLF;
+        }
+  }
   // slow nodes grouped by 128-node region (the unit of work of one warp)
   const long nreg = g.npad / 128;
   out.slow_off.assign(nreg + 1, 0);

@@ -95,6 +95,8 @@ __device__ __forceinline__ void kt_fold(GDev* d, int k) {
   }
 }
 
+struct TlSched;   // work-item claims of the TMA-staged stencil (tdgl_tl.cuh)
+
 template <typename T>
 struct GArgs {
   Grid g;
@@ -159,6 +161,12 @@ struct GArgs {
   T* PW[2];
   T* PB;
   int pstep;
+  // TMA-staged stencil: the work-item claim counters (two sets; stencil
+  // launches that depend programmatically on one another use alternate sets)
+  // and the set of this kernel node (null: each block takes the item of its
+  // block index)
+  TlSched* tls;
+  int tl_par;
 };
 
 template <typename T> __host__ __device__ __forceinline__ double* kry_sj(const GArgs<T>& A) { return A.kry; }
@@ -356,6 +364,16 @@ __device__ __forceinline__ void reduce_parts(const double* part, int nblk, int n
 __device__ __forceinline__ double gfinite(double v) { return isfinite(v) ? v : INFINITY; }
 
 __device__ __forceinline__ bool gdev_ok(const GDev* d) { return d->status == GS_OK; }
+
+// Programmatic dependent launch.  grid_dep_wait: wait until the kernels this
+// launch depends on have completed and their writes are visible (returns at
+// once for a launch without a programmatic dependency).  grid_dep_launch: let
+// the next kernel, when its launch depends on this one programmatically,
+// start its part before its own grid_dep_wait; a kernel calls it only after
+// its own grid_dep_wait, so that every kernel before it has completed when the
+// next one starts.
+__device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void grid_dep_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
 // Stop every loop of the graph with a status (one-block kernels only).
 template <typename T>
@@ -1206,6 +1224,9 @@ __device__ void arn_fold_final(const GArgs<T>& A, int ng, int ja, double* S) {
 template <typename T>
 __global__ void kg_arn_check(GArgs<T> A) {
   __shared__ double ow[kWarps];
+  // the first polynomial step (or the product) may start staging the
+  // linearisation copy while this one-block kernel runs
+  grid_dep_launch();
   GDev* d = A.dev;
   if (!gdev_ok(d)) return;
   const int ja = d->ja;

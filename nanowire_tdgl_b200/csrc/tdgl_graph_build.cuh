@@ -31,9 +31,12 @@ struct Chain {
     if (e == cudaSuccess) last = n;
     return e;
   }
-  // kernel with a __grid_constant__ first parameter (the tensor maps) and the arguments
+  // kernel with a __grid_constant__ first parameter (the tensor maps) and the
+  // arguments; pdl: a programmatic dependency on the previous kernel node (the
+  // kernel may start before that one completes and waits for it with
+  // grid_dep_wait)
   template <class M, class Args>
-  cudaError_t kernel2(const void* fn, dim3 grid, int block, size_t smem, const M& m, Args& args) {
+  cudaError_t kernel2(const void* fn, dim3 grid, int block, size_t smem, const M& m, Args& args, bool pdl = false) {
     cudaKernelNodeParams p{};
     p.func = const_cast<void*>(fn);
     p.gridDim = grid;
@@ -42,6 +45,16 @@ struct Chain {
     void* a[] = {const_cast<M*>(&m), &args};
     p.kernelParams = a;
     cudaGraphNode_t n;
+    if (pdl && last) {
+      cudaError_t e = cudaGraphAddKernelNode(&n, g, nullptr, 0, &p);
+      if (e != cudaSuccess) return e;
+      cudaGraphEdgeData ed{};
+      ed.from_port = cudaGraphKernelNodePortProgrammatic;
+      ed.type = cudaGraphDependencyTypeProgrammatic;
+      e = cudaGraphAddDependencies_v2(g, &last, &n, &ed, 1);
+      if (e == cudaSuccess) last = n;
+      return e;
+    }
     cudaError_t e = cudaGraphAddKernelNode(&n, g, last ? &last : nullptr, last ? 1 : 0, &p);
     if (e == cudaSuccess) last = n;
     return e;
@@ -70,17 +83,19 @@ struct Chain {
 
 // Tangent-linear stencil node (Horner step when poly, else the Arnoldi
 // product): the TMA-staged kernel when tensor maps are given (FP32 vectors,
-// 3-D grids; `chunks` z-chunks), else the kernel that reads global memory.
+// 3-D grids; `chunks` z-chunks; a programmatic dependency on the kernel node
+// before it when tm->pdl), else the kernel that reads global memory.
 template <typename T, bool D3>
-cudaError_t add_tl(Chain& ch, const GArgs<T>& A, const TlMaps* tm, int chunks, bool poly) {
+cudaError_t add_tl(Chain& ch, const GArgs<T>& A, const TlMaps* tm, int chunks, bool poly, int par) {
   GArgs<T> a = A;
+  a.tl_par = par;
   if constexpr (std::is_same<T, float>::value && D3) {
     if (tm) {
-      const void* fn = tm->nx == 2 ? (poly ? (const void*)kg_tl<true, 2> : (const void*)kg_tl<false, 2>)
-                                   : (poly ? (const void*)kg_tl<true, 1> : (const void*)kg_tl<false, 1>);
+      const void* fn = tl_kernel(tm->nx, poly, A.g.kappa_per_node != 0);
       const size_t smem = tl_smem_bytes(tm->nx);
       TDGL_GCK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      return ch.kernel2(fn, dim3(tl_grid_x(A.g.nx, tm->nx), A.arn_gy, chunks), kThreads, smem, *tm, a);
+      return ch.kernel2(fn, dim3(tl_grid_x(A.g.nx, tm->nx), A.arn_gy, chunks), kThreads, smem, *tm, a,
+                        tm->pdl != 0);
     }
   }
   const dim3 tiles(A.arn_gx, A.arn_gy, D3 ? A.g.nz : 1);
@@ -133,7 +148,7 @@ cudaError_t build_trap_graph(GArgs<T> A, const TlMaps* tm, int chunks, cudaGraph
     for (int k = A.poly_deg - 1; k >= 0; --k) {   // p(A) U_ja into PB_ja
       GArgs<T> P = A;
       P.pstep = k;
-      TDGL_GCK((add_tl<T, D3>(ck, P, tm, chunks, true)));
+      TDGL_GCK((add_tl<T, D3>(ck, P, tm, chunks, true, (A.poly_deg - 1 - k) & 1)));
     }
     if (A.apply_dots) {
       const size_t smp = apply_dots_smem<T>(A.kmax);
@@ -141,7 +156,7 @@ cudaError_t build_trap_graph(GArgs<T> A, const TlMaps* tm, int chunks, cudaGraph
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smp));
       TDGL_GCK(ck.kernel((const void*)kg_arn_apply_dots<T, D3>, tiles, kThreads, smp, A));
     } else {
-      TDGL_GCK((add_tl<T, D3>(ck, A, tm, chunks, false)));
+      TDGL_GCK((add_tl<T, D3>(ck, A, tm, chunks, false, A.poly_deg & 1)));
       TDGL_GCK(ck.kernel((const void*)kg_arn_dots<T>, A.nblk_arn, kThreads, smd, A));
     }
   } else {

@@ -13,16 +13,29 @@ cudaError_t graph_build_f32(const GArgs<float>& A, const TlMaps* tm, int chunks,
 // One tangent-linear stencil launch outside the graph (Horner step when poly,
 // else the product): the TMA-staged kernel when tm is given, else the kernel
 // that reads global memory.
-static cudaError_t launch_tl(const GArgs<float>& A, const TlMaps* tm, int chunks, bool poly, cudaStream_t s) {
+// pdl: the launch may start before the previous kernel in the stream
+// completes (only where that kernel writes no linearisation copy: the
+// probe's repeated Arnoldi-step kernels, as in the step graph).
+static cudaError_t launch_tl(const GArgs<float>& A, const TlMaps* tm, int chunks, bool poly, cudaStream_t s,
+                             bool pdl = false) {
   if (A.g.is3d && tm) {
-    const void* fn = tm->nx == 2 ? (poly ? (const void*)kg_tl<true, 2> : (const void*)kg_tl<false, 2>)
-                                 : (poly ? (const void*)kg_tl<true, 1> : (const void*)kg_tl<false, 1>);
+    const void* fn = tl_kernel(tm->nx, poly, A.g.kappa_per_node != 0);
     const size_t smem = tl_smem_bytes(tm->nx);
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     const dim3 grid(tl_grid_x(A.g.nx, tm->nx), A.arn_gy, chunks);
     void* args[] = {const_cast<TlMaps*>(tm), const_cast<GArgs<float>*>(&A)};
-    return cudaLaunchKernel(fn, grid, dim3(kThreads), args, smem, s);
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = dim3(kThreads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = pdl ? 1 : 0;
+    return cudaLaunchKernelExC(&cfg, fn, args);
   }
   const dim3 grid(A.arn_gx, A.arn_gy, A.g.is3d ? A.g.nz : 1);
   if (poly) {
@@ -61,14 +74,20 @@ cudaError_t arnoldi_probe_f32(const GArgs<float>& A, const TlMaps* tm, int chunk
     e = cudaFuncSetAttribute((const void*)kg_arn_apply_dots<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smp);
   const dim3 grid(A.arn_gx, A.arn_gy, A.g.is3d ? A.g.nz : 1);
+  int par = 0;                  // claim-counter set: alternates along the launches of the stencil
   for (int r = 0; r < launches && e == cudaSuccess; ++r) {
     if (kernels & 1) kg_arn_orth<float><<<A.nblk_orth, kThreads, smo, s>>>(A);
     for (int k = (kernels & 16) ? A.poly_deg - 1 : -1; k >= 0 && e == cudaSuccess; --k) {
       GArgs<float> P = A;
       P.pstep = k;
-      e = launch_tl(P, tm, chunks, true, s);
+      P.tl_par = par ^= 1;
+      e = launch_tl(P, tm, chunks, true, s, tm && tm->pdl);
     }
-    if ((kernels & 2) && e == cudaSuccess) e = launch_tl(A, tm, chunks, false, s);
+    if ((kernels & 2) && e == cudaSuccess) {
+      GArgs<float> P = A;
+      P.tl_par = par ^= 1;
+      e = launch_tl(P, tm, chunks, false, s, tm && tm->pdl);
+    }
     if (e != cudaSuccess) break;
     if (kernels & 4) kg_arn_dots<float><<<A.nblk_arn, kThreads, smd, s>>>(A);
     if (kernels & 8) {

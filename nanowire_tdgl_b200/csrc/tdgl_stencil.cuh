@@ -47,6 +47,7 @@ enum : uint8_t {
   NF_HOLEZ = 1u << 3,
   NF_SC0 = 1u << 4,     // sc == 0: pure relaxation -psi/tau
   NF_SCFRAC = 1u << 5,  // sc not in {0, 1}: read the sc array
+  NF_GHOSTLF = 1u << 6, // a face copy of this node lands on a ghost with hole links
 };
 // Per-full-grid-node link flags.
 enum : uint8_t { LF_HX = 1u, LF_HY = 2u, LF_HZ = 4u };

@@ -12,6 +12,8 @@ the product kernel, interior entries back).
 * The TMA-staged kernel (one and two nodes per thread, TDGL_TL_NX) against
   the FP32 kernel that reads global memory (TDGL_TMA=0): 1e-6 relative (same
   arithmetic, contraction order may differ).
+* Holes through the x, y and z faces (ghost nodes with hole links, whose face
+  copies read the link flags): the same bounds.
 * z-chunking of the TMA-staged kernel (TDGL_TL_CHUNKS): bit-identical outputs
   for every chunk count.
 * The 128x128x32 bench device (4 x 16 tiles per plane, the hole): FP32 against
@@ -106,6 +108,49 @@ def test_tma_kernel_against_global_memory_kernel(monkeypatch, periodic, nx):
     plain, _ = _products(dev, X, P, B, "mixed", {"TDGL_TMA": "0"}, monkeypatch)
     assert _rel(tma, want) < 2e-6
     assert _rel(plain, want) < 2e-6
+    assert _rel(tma, plain) < 1e-6
+
+
+def _face_hole_device(tb, periodic):
+    px, py, pz = periodic
+    p = tb.SimulationParameters(Nx=70, Ny=20, Nz=12, hx=0.5, hy=0.5, hz=0.5, kappa=2.0,
+                                periodic_x=px, periodic_y=py, periodic_z=pz)
+    dev = tb.Device(p, applied_field=tb.AppliedField(Bz=0.4, By=0.1, t_on_fraction=1.0))
+    dev.add_hole([(0.0, 3.0), (4.0, 3.0), (4.0, 6.0), (0.0, 6.0)])              # through the x = 0 face
+    dev.add_hole([(20.0, 7.0), (26.0, 7.0), (26.0, 10.0), (20.0, 10.0)], z_range=(0, 5))   # y = Ny and z = 0 faces
+    return dev
+
+
+def _ghosts_with_hole_links(dev):
+    """Ghost nodes (one past a face, inside the other two axes' interior range)
+    that carry hole links: the face copies of the nodes next to them keep those
+    links at zero."""
+    p = dev.params
+    Nx, Ny, Nz = p.Nx, p.Ny, p.Nz
+    hit = np.zeros((Nz + 1) * (Ny + 1) * (Nx + 1), bool)
+    for a in "xyz":
+        hit[np.asarray(getattr(dev.idx, f"hole_{a}_bc_mask"), dtype=np.int64)] = True
+    hit = hit.reshape(Nz + 1, Ny + 1, Nx + 1)
+    ghost = np.zeros_like(hit)
+    ghost[1:Nz, 1:Ny, [0, Nx]] = True
+    ghost[1:Nz, [0, Ny], 1:Nx] = True
+    ghost[[0, Nz], 1:Ny, 1:Nx] = True
+    return int((hit & ghost).sum())
+
+
+@pytest.mark.parametrize("nx", ["1", "2"])
+@pytest.mark.parametrize("periodic", [(False, False, False), (True, True, True)])
+def test_tma_kernel_with_holes_through_faces(monkeypatch, periodic, nx):
+    """Holes that reach the x, y and z faces: the face copies of the output
+    read the ghosts' link flags (the nodes flagged NF_GHOSTLF)."""
+    import nanowire_tdgl_b200 as tb
+    dev = _face_hole_device(tb, periodic)
+    assert _ghosts_with_hole_links(dev) > 0
+    X, P = _state_and_direction(dev, 9)
+    B = (0.05, 0.1, 0.4)
+    tma, want = _products(dev, X, P, B, "mixed", {"TDGL_TL_NX": nx}, monkeypatch)
+    plain, _ = _products(dev, X, P, B, "mixed", {"TDGL_TMA": "0"}, monkeypatch)
+    assert _rel(tma, want) < 2e-6
     assert _rel(tma, plain) < 1e-6
 
 
