@@ -558,6 +558,15 @@ __device__ __forceinline__ V4<double> ld4(const double* p) {
   double2 u = reinterpret_cast<const double2*>(p)[0], v = reinterpret_cast<const double2*>(p)[1];
   return {u.x, u.y, v.x, v.y};
 }
+// The same through L2 only (read once by this kernel: keeps L1 for re-read data).
+__device__ __forceinline__ V4<float> ld4cg(const float* p) {
+  const float4 v = __ldcg(reinterpret_cast<const float4*>(p));
+  return {v.x, v.y, v.z, v.w};
+}
+__device__ __forceinline__ V4<double> ld4cg(const double* p) {
+  const double2 u = __ldcg(reinterpret_cast<const double2*>(p)), v = __ldcg(reinterpret_cast<const double2*>(p) + 1);
+  return {u.x, u.y, v.x, v.y};
+}
 __device__ __forceinline__ void st4(float* p, const double* v) {
   *reinterpret_cast<float4*>(p) = make_float4((float)v[0], (float)v[1], (float)v[2], (float)v[3]);
 }
@@ -1244,13 +1253,14 @@ __global__ void kg_arn_check(GArgs<T> A) {
   if (d->arn_stop) kt_fold(d, KT_ARN_ORTH);
 }
 
-// Projections <Z_ja, U_i> (i <= ja) over the interior entries (imask) in one
-// sweep: at each entry Z is read once and combined with the basis vectors in
-// groups of GGroup<T>::JB whose loads are all in flight together.  Each warp
-// sums its 32 products per vector in T (the vectors' precision); warps and
-// blocks accumulate in double; the partials are folded in two fixed-order
-// levels with the orthogonalisation's ||U_ja||^2 partials, and the last block
-// does the column bookkeeping.
+// Projections <Z_ja, U_i> (i <= ja) over the interior entries (imask): each
+// block sweeps a contiguous range of entries once per group of GGroup<T>::JB
+// basis vectors (whose loads are all in flight together), Z's range staying
+// in L1 between the sweeps.  Threads sum their entries' products per vector in
+// T (the vectors' precision); warps and blocks add those sums in double; the
+// block partials are folded in two fixed-order levels with the
+// orthogonalisation's ||U_ja||^2 partials, and the last block does the column
+// bookkeeping.
 template <typename T>
 __global__ void __launch_bounds__(kThreads, 4) kg_arn_dots(GArgs<T> A) {
   GDev* d = A.dev;
@@ -1266,44 +1276,44 @@ __global__ void __launch_bounds__(kThreads, 4) kg_arn_dots(GArgs<T> A) {
   const T* Z = A.Zb[ja & 1];
   const long vs = A.vs, npf = A.npf, nq = vs / 4;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int t = threadIdx.x; t < kWarps * nd; t += blockDim.x) red[t] = 0.0;
-  __syncthreads();
   constexpr int DG = GGroup<T>::JB;            // vectors per pass: their loads are all in flight at once
-  const long stride = (long)gridDim.x * blockDim.x;
-  // one sweep over the entries: Z is read once per entry and every vector is
-  // combined with it there; the warp adds its 32 products per vector and
-  // lane 0 accumulates the warp's sums in double (all lanes stay in the loop:
-  // its bound is warp-uniform).  The sweep runs from the last entry down: the
-  // orthogonalisation and the product before it swept upwards, so the top
-  // entries of the basis are the ones still in L2 when this kernel starts.
-  const long wq0 = blockIdx.x * (long)blockDim.x + (threadIdx.x & ~31);
-  long mo = (4 * max(nq - 1 - (wq0 + lane), 0L)) % npf;
-  for (long qb = wq0; qb < nq; qb += stride) {
-    const long q = nq - 1 - (qb + lane);
-    const bool ok = q >= 0;
-    const long e = 4 * q;
-    V4<T> z = ok ? ld4(Z + e) : V4<T>{0, 0, 0, 0};
-    if (ok) {
+  // The block's contiguous range of 4-entry groups, swept once per DG
+  // vectors: each thread accumulates its entries' products per vector in T,
+  // the warp adds its 32 sums in double once per vector, and lane 0 keeps the
+  // warp's sums.  Z's range (a few tens of KB) is re-read from L1 by the later
+  // passes; the basis vectors are read through L2 only.
+  const long q0 = nq * blockIdx.x / gridDim.x, q1 = nq * (blockIdx.x + 1) / gridDim.x;
+  const long mo0 = (4 * (q0 + threadIdx.x)) % npf;   // offset within the component (interior mask)
+  const long mstep = 4L * blockDim.x;
+  for (int i0 = 0; i0 <= ja; i0 += DG) {
+    T acc[DG];
+#pragma unroll
+    for (int t = 0; t < DG; ++t) acc[t] = T(0);
+    long mo = mo0;
+    for (long q = q0 + threadIdx.x; q < q1; q += blockDim.x) {
+      const long e = 4 * q;
+      V4<T> z = ld4(Z + e);
       const uchar4 mk = *reinterpret_cast<const uchar4*>(A.imask + mo);
       if (!mk.x) z.a = T(0);
       if (!mk.y) z.b = T(0);
       if (!mk.z) z.c = T(0);
       if (!mk.w) z.d = T(0);
-    }
-    for (int i0 = 0; i0 <= ja; i0 += DG) {
       V4<T> a[DG];
 #pragma unroll
       for (int t = 0; t < DG; ++t)
-        a[t] = (ok && i0 + t <= ja) ? ld4(A.UB + (long)(i0 + t) * vs + e) : V4<T>{0, 0, 0, 0};
+        a[t] = (i0 + t <= ja) ? ld4cg(A.UB + (long)(i0 + t) * vs + e) : V4<T>{0, 0, 0, 0};
 #pragma unroll
-      for (int t = 0; t < DG; ++t) {
-        if (i0 + t > ja) break;                  // warp-uniform: no sums for vectors past ja
-        const T p = warp_sum_t<T>(z.a * a[t].a + z.b * a[t].b + z.c * a[t].c + z.d * a[t].d);
-        if (lane == 0) red[warp * nd + i0 + t] += (double)p;
-      }
+      for (int t = 0; t < DG; ++t)
+        acc[t] = fma(z.a, a[t].a, fma(z.b, a[t].b, fma(z.c, a[t].c, fma(z.d, a[t].d, acc[t]))));
+      mo += mstep;
+      while (mo >= npf) mo -= npf;
     }
-    mo -= 4 * stride;
-    while (mo < 0) mo += npf;
+#pragma unroll
+    for (int t = 0; t < DG; ++t) {
+      if (i0 + t > ja) break;                  // block-uniform: no sums for vectors past ja
+      const double w = warp_sum((double)acc[t]);
+      if (lane == 0) red[warp * nd + i0 + t] = w;
+    }
   }
   __syncthreads();
   for (int s = threadIdx.x; s <= ja; s += blockDim.x) {
