@@ -74,6 +74,9 @@ def parse():
                          "trilayer: the 256x256x64 S/I/S stack, mixed against FP64")
     ap.add_argument("--adj-smax", type=float, default=ADJ["s_max"],
                     help="upper end of the suppression field s(x) of the differentiation workload")
+    ap.add_argument("--probe-no-fill", action="store_true",
+                    help="--arnoldi-probe without the two filling steps (no graph launch in the process, "
+                         "so ncu can replay the probe's kernels; the basis then holds zeros)")
     ap.add_argument("--arnoldi-probe", type=int, default=None, metavar="J",
                     help="diagnostic: time the three Arnoldi-step kernels standalone at basis index J and exit")
     ap.add_argument("--kernel-timers", action="store_true",
@@ -454,7 +457,9 @@ def arnoldi_probe(a):
     a.arnoldi_probe on the workload's context, after two steps that fill the
     basis: the graph's kernels together, then each kernel alone
     (orthogonalisation, product, projections, fused product and projections,
-    the polynomial preconditioner's steps); prints their times."""
+    the polynomial preconditioner's steps), then the Newton-stage kernels
+    (predictor, Newton residual, Newton update over J basis vectors, which
+    overwrite the iterate); prints their times."""
     import torch
     from nanowire_tdgl_b200 import _lib as L
     from nanowire_tdgl_b200.engine import grid_for, stream_handle
@@ -465,15 +470,17 @@ def arnoldi_probe(a):
                       L.TDGL_JVP_ANALYTIC)
     fld = L.Field(0.0, 0.0, w["Bz"], 1.0, 0.5, w["t_stop"], 0, 0)
     x = g.pack(x0)
-    rc, t, cur, st = g.trap_run(x, 0.0, w["dt"], 2, opts, fld)
-    if rc != 0:
-        raise RuntimeError(f"filling steps failed with status {rc}")
+    if not a.probe_no_fill:
+        rc, t, cur, st = g.trap_run(x, 0.0, w["dt"], 2, opts, fld)
+        if rc != 0:
+            raise RuntimeError(f"filling steps failed with status {rc}")
     j = a.arnoldi_probe
     reps = max(a.steps, 1)
     res = {}
     deg = g.poly_degree
     for name, mask in (("graph", 0), ("orthogonalisation", 1), ("product", 2), ("projections", 4),
-                       ("product_and_projections", 8), ("polynomial_steps", 16)):
+                       ("product_and_projections", 8), ("polynomial_steps", 16), ("predict", 32),
+                       ("newton_residual", 64), ("newton_update", 128)):
         if mask == 16 and deg == 0:
             continue
         L.check(g.lib.tdgl_arnoldi_probe(g.handle, j, 2, mask, stream_handle()), "tdgl_arnoldi_probe")

@@ -327,7 +327,9 @@ int tdgl_profile(tdgl_ctx* ctx, uint64_t* out, int64_t n, int32_t reset);
  * workspace holds, without the Krylov bookkeeping; synchronises the stream.
  * kernels selects what runs (bit 0 orthogonalisation, bit 1 product, bit 2
  * projections, bit 3 fused product and projections, bit 4 the polynomial
- * preconditioner's steps; 0 = the graph's own).
+ * preconditioner's steps, bits 5-7 the Newton-stage kernels: predictor,
+ * Newton residual, Newton update over ja basis vectors, which overwrite the
+ * iterate; 0 = the graph's own).
  * For timing and profiling the kernels alone.  No reference counterpart. */
 int tdgl_arnoldi_probe(tdgl_ctx* ctx, int32_t ja, int32_t launches, int32_t kernels, tdgl_stream_t stream);
 

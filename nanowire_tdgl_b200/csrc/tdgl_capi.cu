@@ -1393,6 +1393,11 @@ extern "C" int tdgl_arnoldi_probe(tdgl_ctx* c, int32_t ja, int32_t launches, int
   if (ja < 0 || ja > c->kmax) return fail(TDGL_EINVAL, "ja must lie in [0, kmax]");
   c->has_clock = false;
   TDGL_CUDA(cudaMemcpyAsync(&c->gdev->ja, &ja, sizeof(int), cudaMemcpyHostToDevice, s));
+  // the limit of the device-side waits (a graph launch writes it; the probe
+  // may be the context's first launch)
+  TDGL_CUDA(cudaMemcpyAsync(&c->gdev->wait_ns, &c->wait_ns, sizeof(c->wait_ns), cudaMemcpyHostToDevice, s));
+  if (kernels & 128)                // the Newton update combines ja basis vectors
+    TDGL_CUDA(cudaMemcpyAsync(&c->gdev->j, &ja, sizeof(int), cudaMemcpyHostToDevice, s));
   cudaError_t e;
   if (c->precision == TDGL_MIXED) {
     GArgs<float> A = make_gargs<float>(c);

@@ -380,6 +380,7 @@ template <typename T>
 __device__ __forceinline__ void abort_all(const GArgs<T>& A, int status) {
   if (threadIdx.x == 0) {
     if (A.dev->status == GS_OK) A.dev->status = status;
+    if (A.standalone) return;      // a launch outside the graph has no conditional nodes to stop
     cudaGraphSetConditional(A.h_krylov, 0);
     cudaGraphSetConditional(A.h_newton, 0);
     cudaGraphSetConditional(A.h_step, 0);
@@ -422,6 +423,42 @@ __global__ void __launch_bounds__(kThreads) kg_prepare(GArgs<T> A) {
   kt_end(A.dev, KT_PREPARE);
 }
 
+// Tiles of the interior (3-D grids): 32 x 8 nodes of one plane, planes
+// 1 .. nz, so that the grid kernels take node coordinates from the tile with
+// no division per node.  Index q = tile * kThreads + thread in the tile.
+struct EffTiles {
+  int gx, gxy, n;
+  __device__ __forceinline__ explicit EffTiles(const Grid& g)
+      : gx((g.nx + 31) / 32), gxy(((g.nx + 31) / 32) * ((g.ny + 7) / 8)), n(gxy * g.nz) {}
+  // node of index q: false past the grid's last column or row
+  __device__ __forceinline__ bool node(const Grid& g, int q, int& i, int& j, int& k) const {
+    const int t = q / kThreads, l = q - t * kThreads;
+    const int z = t / gxy, r = t - z * gxy;
+    const int ty = r / gx;
+    k = 1 + z;
+    j = 1 + 8 * ty + (l >> 5);
+    i = 1 + 32 * (r - ty * gx) + (l & 31);
+    return i <= g.nx && j <= g.ny;
+  }
+};
+
+// node_coef<double> with the uniform kappa^2 / h^2 of the launch (no division
+// per node unless kappa varies per node).
+template <typename T>
+__device__ __forceinline__ NodeCoef<double> node_coef_u(const GArgs<T>& A, const Grid& g, int n, uint8_t nf) {
+  if (g.kappa_per_node) return node_coef<double>(g, n, nf);
+  NodeCoef<double> nc;
+  nc.cx = A.cxu;
+  nc.cy = A.cyu;
+  nc.cz = A.czu;
+  nc.material = g.has_material != 0;
+  if (!nc.material) nc.sc = 1.0;
+  else if (nf & NF_SCFRAC) nc.sc = g.scint[n];
+  else nc.sc = (nf & NF_SC0) ? 0.0 : 1.0;
+  set_ih(g, nc);
+  return nc;
+}
+
 // Predictor: f = rhs(Xn); Xi = Xn + dt f; G = Xn + dt/2 f (integrators.py:156-158);
 // effective copies of Xi (FP64, and in T for the Jacobian products).
 template <typename T, bool D3>
@@ -431,14 +468,7 @@ __global__ void __launch_bounds__(kThreads, 3) kg_predict(GArgs<T> A) {
   kt_begin(A.dev, KT_PREDICT);
   const Grid& g = A.g;
   const double dt = d->dta, czxy = d->czxy, cyzx = d->cyzx, cxyz = d->cxyz;
-  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < g.n; n += gridDim.x * blockDim.x) {
-    int i, j, k;
-    node_ijk(g, n, i, j, k);
-    const uint8_t nf = g.nflags[n];
-    NodeCoef<double> nc = node_coef<double>(g, n, nf);
-    NbE<double, double> X{A.En, A.npf, full_index(g, i, j, k), g.mj, g.mk};
-    double o[5];
-    rhs_body<double, D3>(g, X, nc, nf, o);
+  auto node = [&](int n, int i, int j, int k, const double o[5]) {
     double xi[5] = {0, 0, 0, 0, 0};
 #pragma unroll
     for (int c = 0; c < (D3 ? 5 : 4); ++c) {
@@ -450,6 +480,24 @@ __global__ void __launch_bounds__(kThreads, 3) kg_predict(GArgs<T> A) {
     }
     write_eff<double, D3>(g, A.Ei, A.npf, i, j, k, xi, czxy, cyzx, cxyz);
     if ((void*)A.XLe != (void*)A.Ei) write_eff<T, D3>(g, A.XLe, A.npf, i, j, k, xi, czxy, cyzx, cxyz);
+  };
+  const EffTiles tl(g);
+  const int nt = D3 ? tl.n * kThreads : g.n;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nt; q += gridDim.x * blockDim.x) {
+    int i, j, k, n;
+    if constexpr (D3) {
+      if (!tl.node(g, q, i, j, k)) continue;
+      n = dix(g, i, j, k);
+    } else {
+      n = q;
+      node_ijk(g, n, i, j, k);
+    }
+    const uint8_t nf = g.nflags[n];
+    const NodeCoef<double> nc = node_coef_u(A, g, n, nf);
+    const NbE<double, double> X{A.En, A.npf, full_index(g, i, j, k), g.mj, g.mk};
+    double o[5];
+    rhs_body<double, D3>(g, X, nc, nf, o);
+    node(n, i, j, k, o);
   }
   kt_end(A.dev, KT_PREDICT);
 }
@@ -464,14 +512,7 @@ __global__ void __launch_bounds__(kThreads, 3) kg_newton_rhs(GArgs<T> A) {
   const Grid& g = A.g;
   const double dt = d->dta;
   double acc[3] = {0.0, 0.0, 0.0};
-  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < g.n; n += gridDim.x * blockDim.x) {
-    int i, j, k;
-    node_ijk(g, n, i, j, k);
-    const uint8_t nf = g.nflags[n];
-    NodeCoef<double> nc = node_coef<double>(g, n, nf);
-    NbE<double, double> X{A.Ei, A.npf, full_index(g, i, j, k), g.mj, g.mk};
-    double o[5];
-    rhs_body<double, D3>(g, X, nc, nf, o);
+  auto node = [&](int n, int i, int j, int k, const double o[5]) {
     double gv[5] = {0, 0, 0, 0, 0}, r[5] = {0, 0, 0, 0, 0};
 #pragma unroll
     for (int c = 0; c < (D3 ? 5 : 4); ++c) {
@@ -491,6 +532,24 @@ __global__ void __launch_bounds__(kThreads, 3) kg_newton_rhs(GArgs<T> A) {
     acc[2] = fmax(acc[2], m);
     if (A.fused) write_eff<T, D3, true>(g, A.UB, A.npf, i, j, k, r, 0.0, 0.0, 0.0);
     else write_eff<T, D3>(g, A.VE, A.npf, i, j, k, r, 0.0, 0.0, 0.0);
+  };
+  const EffTiles tl(g);
+  const int nt = D3 ? tl.n * kThreads : g.n;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nt; q += gridDim.x * blockDim.x) {
+    int i, j, k, n;
+    if constexpr (D3) {
+      if (!tl.node(g, q, i, j, k)) continue;
+      n = dix(g, i, j, k);
+    } else {
+      n = q;
+      node_ijk(g, n, i, j, k);
+    }
+    const uint8_t nf = g.nflags[n];
+    const NodeCoef<double> nc = node_coef_u(A, g, n, nf);
+    const NbE<double, double> X{A.Ei, A.npf, full_index(g, i, j, k), g.mj, g.mk};
+    double o[5];
+    rhs_body<double, D3>(g, X, nc, nf, o);
+    node(n, i, j, k, o);
   }
   const bool mx[3] = {false, false, true};
   block_partials<3>(acc, mx, A.part_nrhs, A.nblk);
@@ -753,10 +812,19 @@ __global__ void __launch_bounds__(kThreads, 3) kg_update_fused(GArgs<T> A) {
   const T* UBase = A.poly_deg > 0 ? A.PB : A.UB;
   const double czxy = d->czxy, cyzx = d->cyzx, cxyz = d->cxyz;
   double acc[1] = {0.0};
-  // basis on the full grid: one node per thread
-  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < g.n; n += gridDim.x * blockDim.x) {
-    int i, j, k;
-    node_ijk(g, n, i, j, k);
+  // basis on the full grid: one node per thread (3-D: tiles of 32 x 8 nodes
+  // of one plane, no division per node)
+  const EffTiles tl(g);
+  const int nt = D3 ? tl.n * kThreads : g.n;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nt; q += gridDim.x * blockDim.x) {
+    int i, j, k, n;
+    if constexpr (D3) {
+      if (!tl.node(g, q, i, j, k)) continue;
+      n = dix(g, i, j, k);
+    } else {
+      n = q;
+      node_ijk(g, n, i, j, k);
+    }
     const long m = full_index(g, i, j, k);
     double s[NC], v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
 #pragma unroll

@@ -56,7 +56,9 @@ cudaError_t product_f32(const GArgs<float>& A, const TlMaps* tm, int chunks, cud
 // Diagnostic: `launches` standalone Arnoldi steps.  kernels: bit 0 the
 // orthogonalisation, bit 1 the product, bit 2 the projections, bit 3 the fused
 // product and projections, bit 4 the polynomial preconditioner's steps (its
-// degree, before the product); 0 = the kernels of this context's graph.
+// degree, before the product), bits 5-7 the Newton-stage kernels (predictor,
+// Newton residual, Newton update over ja basis vectors; they overwrite the
+// iterate); 0 = the kernels of this context's graph.
 cudaError_t arnoldi_probe_f32(const GArgs<float>& A, const TlMaps* tm, int chunks, int launches, int kernels,
                               cudaStream_t s) {
   const size_t smo = (size_t)(A.kmax + 1) * sizeof(double);
@@ -93,6 +95,18 @@ cudaError_t arnoldi_probe_f32(const GArgs<float>& A, const TlMaps* tm, int chunk
     if (kernels & 8) {
       if (A.g.is3d) kg_arn_apply_dots<float, true><<<grid, kThreads, smp, s>>>(A);
       else kg_arn_apply_dots<float, false><<<grid, kThreads, smp, s>>>(A);
+    }
+    if (kernels & 32) {
+      if (A.g.is3d) kg_predict<float, true><<<A.nblk, kThreads, 0, s>>>(A);
+      else kg_predict<float, false><<<A.nblk, kThreads, 0, s>>>(A);
+    }
+    if (kernels & 64) {
+      if (A.g.is3d) kg_newton_rhs<float, true><<<A.nblk, kThreads, 0, s>>>(A);
+      else kg_newton_rhs<float, false><<<A.nblk, kThreads, 0, s>>>(A);
+    }
+    if (kernels & 128) {
+      if (A.g.is3d) kg_update_fused<float, true><<<A.nblk, kThreads, 0, s>>>(A);
+      else kg_update_fused<float, false><<<A.nblk, kThreads, 0, s>>>(A);
     }
     e = cudaGetLastError();
   }

@@ -50,6 +50,18 @@ cudaError_t arnoldi_probe_f64(const GArgs<double>& A, int launches, int kernels,
       else kg_arn_apply<double, false><<<grid, kThreads, 0, s>>>(A);
     }
     if (kernels & 4) kg_arn_dots<double><<<A.nblk_arn, kThreads, smd, s>>>(A);
+    if (kernels & 32) {
+      if (A.g.is3d) kg_predict<double, true><<<A.nblk, kThreads, 0, s>>>(A);
+      else kg_predict<double, false><<<A.nblk, kThreads, 0, s>>>(A);
+    }
+    if (kernels & 64) {
+      if (A.g.is3d) kg_newton_rhs<double, true><<<A.nblk, kThreads, 0, s>>>(A);
+      else kg_newton_rhs<double, false><<<A.nblk, kThreads, 0, s>>>(A);
+    }
+    if (kernels & 128) {
+      if (A.g.is3d) kg_update_fused<double, true><<<A.nblk, kThreads, 0, s>>>(A);
+      else kg_update_fused<double, false><<<A.nblk, kThreads, 0, s>>>(A);
+    }
     if (kernels & 8) {
       if (A.g.is3d) kg_arn_apply_dots<double, true><<<grid, kThreads, smp, s>>>(A);
       else kg_arn_apply_dots<double, false><<<grid, kThreads, smp, s>>>(A);

@@ -9,6 +9,8 @@ first waits, with its own bound, for the copies it has in flight), the call
 returns TDGL_ETIMEOUT and later kernels of the launch return at once.  The
 loop cap bounds the conditional-loop iterations of one step-graph launch.
 Restoring the defaults, the same context then steps exactly as a fresh one.
+Kernels launched outside the graph (the Arnoldi-step probe) record a
+failure's status without touching the graph's conditional nodes.
 The reference has no device waits; its failure conventions (a failed solve
 is an exception, src/tdgl3d/solvers/integrators.py:186-197) are kept by the
 Python layer for the codes it maps.
@@ -99,4 +101,28 @@ def test_staged_stencil_wait_limit():
     assert e.value.status == L.TDGL_ETIMEOUT
     g.set_limits()
     got = g.jvp(x, p, 0.1, "krylov", B=B)
+    assert torch.equal(got, want)
+
+
+def test_standalone_kernels_after_a_wait_runs_out():
+    """Standalone launches (the Arnoldi-step probe, outside any graph) on a
+    fresh context whose wait limit runs out: the staged stencil records the
+    timeout, and the projections that follow only record the status (outside
+    the graph there are no conditional nodes to stop).  The context then
+    steps exactly as a fresh one."""
+    from nanowire_tdgl_b200 import _lib as L
+    from nanowire_tdgl_b200.engine import stream_handle
+    mk, x0, opts, fld = _setup("mixed")
+    ref = mk()
+    rc, want = _run(ref, x0, opts, fld)
+    assert rc == L.TDGL_OK
+    g = mk()
+    g.set_limits(wait_ns=1)
+    # the graph's Arnoldi-step kernels at basis index 2: orthogonalisation,
+    # polynomial steps, product, projections
+    L.check(g.lib.tdgl_arnoldi_probe(g.handle, 2, 1, 0, stream_handle()), "tdgl_arnoldi_probe")
+    torch.cuda.synchronize()
+    g.set_limits()
+    rc, got = _run(g, x0, opts, fld)
+    assert rc == L.TDGL_OK
     assert torch.equal(got, want)
