@@ -321,6 +321,10 @@ def run_ours(a, rank, world):
         "data": "synthetic (seeded psi0 noise, phi0 = 0; no dataset involved)",
         "config": {"workload": WORKLOAD_NAME, "precision": a.precision, "jvp": jvp, "krylov": a.krylov,
                    "preconditioner": f"Chebyshev polynomial, degree {poly_deg}" if poly_deg else "none",
+                   "krylov_stop": ("tol_gcr relative, or once ||r||_2 <= 0.1 tol_f (forcing term; the Newton "
+                                   "test is unchanged)"
+                                   if (jvp == "analytic" and a.krylov == "gmres"
+                                       and os.environ.get("TDGL_FORCING", "1") != "0") else "tol_gcr relative"),
                    "n_interior": n_int,
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": ("inputs larger than L2: each step touches ~0.3 GB (FP64 state, iterate, gamma and f, "

@@ -48,6 +48,7 @@ __global__ void kg_adj_init_fin(GArgs<double> A) {
   if (!isfinite(d->rho0)) { abort_all(A, GS_NONFINITE); return; }
   d->j = 0;
   d->rho = d->rho0;
+  d->tol_lin = d->tol_gcr;         // the adjoint solves stop at tol_gcr relative
   kry_gv(A)[0] = d->rho0;
   kry_sj(A)[0] = d->rho0 > 0.0 ? 1.0 / d->rho0 : 0.0;
   cudaGraphSetConditional(A.h_krylov, d->rho0 > 0.0 ? 1 : 0);

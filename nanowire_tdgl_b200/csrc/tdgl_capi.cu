@@ -161,6 +161,7 @@ struct tdgl_ctx {
   uint32_t* deadmask = nullptr;   // per interior node: dead links read by the Arnoldi product
   uint8_t* ldead = nullptr;       // per full-grid node: its dead links (TMA-staged stencil)
   TlSched* tls = nullptr;         // the TMA-staged stencil's two sets of work-item claim counters
+  int forcing = 1;                // forcing term of the analytic-product GMRES solves (TDGL_FORCING=0: off)
   // TMA-staged tangent-linear stencil (FP32 vectors, 3-D grids): tensor maps of
   // the staged vectors and the z-chunks per tile column
   TlMaps tlm{};
@@ -738,6 +739,7 @@ static GArgs<T> make_gargs(tdgl_ctx* c) {
   A.ldead = c->ldead;
   A.tls = c->tl_on ? c->tls : nullptr;
   A.tl_par = 0;
+  A.forcing = c->forcing;
   A.ntiles = c->ntiles;
   A.ngroups = c->ngroups;
   A.gpart = c->gpart;
@@ -974,6 +976,9 @@ static int ensure_graph(tdgl_ctx* c, int v) {
     if ((rc = ctx_alloc(c, (void**)&c->gclk, 2 * sizeof(double)))) return rc;
     const char* pe = std::getenv("TDGL_PROFILE");
     c->gprof = pe && pe[0] && pe[0] != '0';
+    // forcing term of the analytic-product GMRES solves (on; TDGL_FORCING=0
+    // keeps every solve at tol_gcr)
+    if (const char* e = std::getenv("TDGL_FORCING")) c->forcing = e[0] == '0' ? 0 : 1;
     c->gws_ready = true;
   }
   if (v == 1 && (rc = ensure_arnoldi_ws(c))) return rc;
@@ -982,11 +987,13 @@ static int ensure_graph(tdgl_ctx* c, int v) {
     GArgs<float> A = make_gargs<float>(c);
     A.fused = v;
     if (!v) A.poly_deg = 0;
+    if (!v) A.forcing = 0;
     e = graph_build_f32(A, (v && c->tl_on) ? &c->tlm : nullptr, c->tl_chunks, &c->graph[v], &c->gexec[v]);
   } else {
     GArgs<double> A = make_gargs<double>(c);
     A.fused = v;
     if (!v) A.poly_deg = 0;
+    if (!v) A.forcing = 0;
     e = graph_build_f64(A, &c->graph[v], &c->gexec[v]);
   }
   if (e != cudaSuccess) {
@@ -1128,6 +1135,7 @@ extern "C" int tdgl_adjoint_solve(tdgl_ctx* c, const double* x, const double* b,
   }
   if (!c->adj_exec) {
     GArgs<double> A = make_gargs<double>(c);
+    A.forcing = 0;
     A.ax = c->adj;
     A.ab = c->adj + L;
     A.amu = c->adj + 2 * L;
