@@ -43,14 +43,14 @@ WORKLOAD_NAME = ("trapezoidal step, 128x128x32-cell film (499,999 interior nodes
 HBM_FALLBACK_GBS = 6650.0
 WORKLOAD_N_INTERIOR = 127 * 127 * 31
 # DRAM bytes per algorithmic byte of the GMRES step graph on the 128x128x32
-# workload at the default preconditioner degree (5), from a graph-level ncu
+# workload at the default preconditioner degree (8), from a graph-level ncu
 # capture (dram__bytes_read.sum + dram__bytes_write.sum) of the timed 2-step
 # launch of `bench.py --steps 2 --warmup 3 --no-fp64 --no-e2e
-# --no-cpu-baseline --no-forms`: 1.327 GB read + 1.814 GB written = 3.140 GB
-# against 8.064 GB algorithmic.  The stencil launches' vectors stay in L2;
+# --no-cpu-baseline --no-forms`: 0.872 GB read + 1.455 GB written = 2.327 GB
+# against 7.447 GB algorithmic.  The stencil launches' vectors stay in L2;
 # the projections read most of the basis from DRAM.
-DRAM_PER_ALG_BYTE = 0.3894
-DRAM_RATIO_DEGREE = 5
+DRAM_PER_ALG_BYTE = 0.3124
+DRAM_RATIO_DEGREE = 8
 
 
 def parse():
@@ -335,7 +335,7 @@ def run_ours(a, rank, world):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "traffic_note": traffic_note, "peak_kind": peak_kind,
                      "limiter": ("the roofline is HBM (streaming stencils, no contraction), but the preconditioned "
-                                 "step's working set stays mostly in L2 (DRAM traffic ~0.39 x the algorithmic "
+                                 "step's working set stays mostly in L2 (DRAM traffic ~0.31 x the algorithmic "
                                  "bytes) and the step is bound by the tangent-linear stencil launches, which are "
                                  "latency- and issue-bound (~455 instructions per node at ~42% issue-active with 16 "
                                  "warps per SM; the polynomial steps and products take ~2/3 of the step)"),

@@ -275,7 +275,7 @@ int tdgl_ctx_set_limits(tdgl_ctx* ctx, int64_t wait_ns, int64_t loop_cap);
  * [1 - dt/2, 1 + dt/2 rho], rho a Gershgorin bound of J; the Newton
  * correction is p(A) times the Krylov combination, so the stop test and the
  * solution are those of the unpreconditioned system.  0 turns it off, -1
- * restores the default (5, or TDGL_POLY_DEGREE).  The finite-difference
+ * restores the default (8, or TDGL_POLY_DEGREE).  The finite-difference
  * (reference) form never uses it.  The graph is rebuilt at the next launch;
  * TDGL_EINVAL while a launch is pending.  No reference counterpart (the
  * reference's GCR is unpreconditioned). */
