@@ -520,7 +520,7 @@ __global__ void __launch_bounds__(kThreads, 3) kg_predict(GArgs<T> A) {
     }
     const uint8_t nf = g.nflags[n];
     const NodeCoef<double> nc = node_coef_u(A, g, n, nf);
-    const NbE<double, double> X{A.En, A.npf, full_index(g, i, j, k), g.mj, g.mk};
+    const NbEro<double> X{A.En, A.npf, full_index(g, i, j, k), g.mj, g.mk};   // En: read only in this kernel
     double o[5];
     rhs_body<double, D3>(g, X, nc, nf, o);
     node(n, i, j, k, o);
@@ -572,7 +572,7 @@ __global__ void __launch_bounds__(kThreads, 3) kg_newton_rhs(GArgs<T> A) {
     }
     const uint8_t nf = g.nflags[n];
     const NodeCoef<double> nc = node_coef_u(A, g, n, nf);
-    const NbE<double, double> X{A.Ei, A.npf, full_index(g, i, j, k), g.mj, g.mk};
+    const NbEro<double> X{A.Ei, A.npf, full_index(g, i, j, k), g.mj, g.mk};   // Ei: read only in this kernel
     double o[5];
     rhs_body<double, D3>(g, X, nc, nf, o);
     node(n, i, j, k, o);
@@ -856,20 +856,21 @@ __global__ void __launch_bounds__(kThreads, 3) kg_update_fused(GArgs<T> A) {
 #pragma unroll
     for (int c = 0; c < NC; ++c) s[c] = 0.0;
     int i0 = 0;
+    // the basis is read only in this kernel: read-only loads
     for (; i0 + 4 <= nk; i0 += 4) {
       const T* U = UBase + (long)i0 * A.vs + m;
       const double c0 = cj[i0], c1 = cj[i0 + 1], c2 = cj[i0 + 2], c3 = cj[i0 + 3];
 #pragma unroll
       for (int c = 0; c < NC; ++c) {
         const long e = (long)c * A.npf;
-        s[c] += c0 * (double)U[e] + c1 * (double)U[A.vs + e] + c2 * (double)U[2 * A.vs + e] +
-                c3 * (double)U[3 * A.vs + e];
+        s[c] += c0 * (double)__ldg(U + e) + c1 * (double)__ldg(U + A.vs + e) + c2 * (double)__ldg(U + 2 * A.vs + e) +
+                c3 * (double)__ldg(U + 3 * A.vs + e);
       }
     }
     for (; i0 < nk; ++i0) {
       const T* U = UBase + (long)i0 * A.vs + m;
 #pragma unroll
-      for (int c = 0; c < NC; ++c) s[c] += cj[i0] * (double)U[(long)c * A.npf];
+      for (int c = 0; c < NC; ++c) s[c] += cj[i0] * (double)__ldg(U + (long)c * A.npf);
     }
 #pragma unroll
     for (int c = 0; c < NC; ++c) {
