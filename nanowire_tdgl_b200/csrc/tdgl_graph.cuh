@@ -99,10 +99,12 @@ __device__ __forceinline__ void kt_fold(GDev* d, int k) {
 struct TlSched;   // work-item claims of the TMA-staged stencil (tdgl_tl.cuh)
 
 // Forcing term: the relative residual at which the first Krylov solve of a
-// step stops at the latest (measured on the 128x128x32 film: 1e-6, 1e-4, 1e-3,
-// 1e-2 give 201, 175, 170, 163 Krylov iterations over 20 steps and 40, 41, 41,
-// 41 Newton iterations).
-constexpr double kEtaFirst = 1e-3;
+// step stops at the latest (Eisenstat and Walker's usual starting value).
+// Measured with the degree-8 preconditioner, Krylov / Newton iterations and
+// steps/s: 128x128x32 film over 20 steps, 1e-3: 117 / 41 / 713.3, 1e-2:
+// 117 / 41 / 713.7, 1e-1: 109 / 44 / 738.1; 256x256x64 trilayer, 1e-3:
+// 341 / 60 / 45.66, 1e-2: 326 / 60 / 47.44, 1e-1: 314 / 60 / 48.98.
+constexpr double kEtaFirst = 1e-1;
 
 template <typename T>
 struct GArgs {
