@@ -269,13 +269,13 @@ int tdgl_ctx_set_blocks(tdgl_ctx* ctx, int32_t stream_blocks, int32_t krylov_blo
  * defaults (5 s; a cap derived from max_steps, newton_max_iter and kmax).
  * The context stays usable after either limit has run out. */
 int tdgl_ctx_set_limits(tdgl_ctx* ctx, int64_t wait_ns, int64_t loop_cap);
-/* Degree (0 to 8) of the polynomial right preconditioner of the GMRES solves
+/* Degree (0 to 12) of the polynomial right preconditioner of the GMRES solves
  * with analytic Jacobian products: GMRES runs on A p(A), A = I - dt/2 J,
  * p the Chebyshev-iteration polynomial of that degree for the interval
  * [1 - dt/2, 1 + dt/2 rho], rho a Gershgorin bound of J; the Newton
  * correction is p(A) times the Krylov combination, so the stop test and the
  * solution are those of the unpreconditioned system.  0 turns it off, -1
- * restores the default (8, or TDGL_POLY_DEGREE).  The finite-difference
+ * restores the default (10, or TDGL_POLY_DEGREE).  The finite-difference
  * (reference) form never uses it.  The graph is rebuilt at the next launch;
  * TDGL_EINVAL while a launch is pending.  No reference counterpart (the
  * reference's GCR is unpreconditioned). */

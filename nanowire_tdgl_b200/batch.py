@@ -183,7 +183,7 @@ class BatchedTrapezoidal:
         the fastest.  States, clocks and counters are restored.  Returns
         {candidate: ms}.  (Stiffer instances, larger kappa^2 dt / h^2, gain
         from the higher degree: on the 64-instance workload degree 5 stepped
-        9 % faster than degree 3; 8 is the single-instance default.)"""
+        9 % faster than degree 3; 10 is the single-instance default.)"""
         snap = self.snapshot()
         times = {}
         for cand in candidates:

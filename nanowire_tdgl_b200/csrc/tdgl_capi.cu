@@ -44,10 +44,11 @@ static constexpr long kProfLen = 64 + 2 * 1024;
 // upper bound of the step graph's blocks per SM (its partial-sum buffers are sized for it)
 static constexpr int kMaxBlocksPerSm = 8;
 // default degree of the polynomial preconditioner (analytic-product GMRES):
-// the highest; on the 128x128x32 film with the forcing term degrees 3-8 gave
-// 604.7, 640.7, 671.3, 685.4, 694.4, 706.5 steps/s, on the 256x256x64
-// trilayer 5-8 gave 42.7, 44.3, 45.3, 45.5 steps/s
-static constexpr int kPolyDefault = 8;
+// on the 128x128x32 film with the forcing term degrees 3-8 gave 604.7, 640.7,
+// 671.3, 685.4, 694.4, 706.5 steps/s, and on the final stencil build degrees
+// 8, 10, 12 gave 737.0, 809.1, 733.1; on the 256x256x64 trilayer degrees 8,
+// 10, 12 gave 48.74, 51.41, 52.13 steps/s
+static constexpr int kPolyDefault = 10;
 // default limit of one bounded device wait (grid barrier, staged-copy mbarrier)
 static constexpr unsigned long long kWaitDefaultNs = 5000000000ull;
 
@@ -1239,7 +1240,7 @@ extern "C" int tdgl_ctx_set_blocks(tdgl_ctx* c, int32_t stream_blocks, int32_t k
 
 extern "C" int tdgl_ctx_set_poly(tdgl_ctx* c, int32_t degree) {
   if (!c) return fail(TDGL_EINVAL, "null argument");
-  if (degree < -1 || degree > kPolyMax) return fail(TDGL_EINVAL, "polynomial degree must lie in [-1, 8]");
+  if (degree < -1 || degree > kPolyMax) return fail(TDGL_EINVAL, "polynomial degree must lie in [-1, 12]");
   if (c->npend) return fail(TDGL_EINVAL, "a launch of this context has not been collected");
   c->poly_req = degree;
   if (c->UB) c->poly_deg = poly_setting(c);

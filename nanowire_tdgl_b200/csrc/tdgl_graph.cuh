@@ -45,7 +45,7 @@ enum GStatus : int {
 constexpr int kKTypes = 16;   // slots of the per-kernel timers
 
 // Device control block of the graph executor.
-constexpr int kPolyMax = 8;   // highest degree of the polynomial preconditioner
+constexpr int kPolyMax = 12;  // highest degree of the polynomial preconditioner
 
 struct GDev {
   // inputs for one launch

@@ -87,7 +87,7 @@ def test_poly_setting_is_validated(tb):
     from nanowire_tdgl_b200._lib import TDGLError
     dev, _ = _case(tb)
     g = _grid(dev, "mixed")
-    for bad in (-2, 9):
+    for bad in (-2, 13):
         with pytest.raises(TDGLError):
             g.set_poly(bad)
     g.set_poly(5)
@@ -95,4 +95,4 @@ def test_poly_setting_is_validated(tb):
     g.set_poly(0)
     assert g.poly_degree == 0
     g.set_poly(-1)
-    assert 0 <= g.poly_degree <= 8
+    assert 0 <= g.poly_degree <= 12
