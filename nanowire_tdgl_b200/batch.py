@@ -56,6 +56,25 @@ def assign_streams(sizes: Sequence[int], n_streams: int) -> tuple[list, list]:
     return queues, order
 
 
+def instance_field(applied_field, t_stop: float, schedule: bool) -> L.Field:
+    """Device field of one instance.  Without ``schedule``: the constant
+    (Bx, By, Bz) of its ``AppliedField`` at every step.  With it: the
+    ``AppliedField`` schedule against ``t_stop`` (zero at t <= 0 and after
+    t_stop * t_on_fraction, the optional ramp), evaluated at each step's
+    start as the reference's step loop does (src/tdgl3d/solvers/
+    integrators.py:150-153, physics/applied_field.py:42-56); a Python
+    ``field_func`` cannot be evaluated on the device (ValueError)."""
+    af = applied_field
+    if not schedule:
+        return L.Field(float(af.Bx), float(af.By), float(af.Bz), 1.0, 0.0, float(t_stop), 0, 1)
+    if getattr(af, "field_func", None) is not None:
+        raise ValueError("field_schedule needs an AppliedField without field_func")
+    if not math.isfinite(t_stop):
+        raise ValueError("field_schedule needs a finite t_stop")
+    return L.Field(float(af.Bx), float(af.By), float(af.Bz), float(af.t_on_fraction), float(af.ramp_fraction),
+                   float(t_stop), int(bool(af.ramp)), 0)
+
+
 def launch_blocks(n: int, nodes_per_thread: Optional[int], sms: int) -> tuple[int, int]:
     """(grid-stride blocks, Arnoldi blocks) of an instance of n interior
     nodes: the single-instance default (8 and 5 blocks per SM) for None, else
@@ -69,14 +88,18 @@ def launch_blocks(n: int, nodes_per_thread: Optional[int], sms: int) -> tuple[in
 class BatchedTrapezoidal:
     """Trapezoidal stepping of ``devices`` (``Device`` objects, distinct) from
     the reference-layout states ``x0s``, each with its device's constant
-    applied field (Bx, By, Bz of its ``AppliedField``)."""
+    applied field (Bx, By, Bz of its ``AppliedField``), or, with
+    ``field_schedule``, with its ``AppliedField`` schedule against
+    ``t_stop`` as ``solve`` applies it (``instance_field``)."""
 
     def __init__(self, devices: Sequence, x0s: Sequence, dt: float, *, t_start: float = 0.0,
                  t_stop: float = 1e30, precision: str = "mixed", kmax: int = 64, newton_tol_f: float = 1e-8,
                  newton_tol_dx: float = 1e-3, newton_max_iter: int = 20, tol_gcr: float = 1e-6,
-                 eps_mf: float = 1e-4, adaptive: bool = True, dt_min: float = 1e-8, n_streams: int = 32):
+                 eps_mf: float = 1e-4, adaptive: bool = True, dt_min: float = 1e-8, n_streams: int = 32,
+                 field_schedule: bool = False):
         if len({id(d) for d in devices}) != len(devices):
             raise ValueError("every instance needs its own Device object")
+        fields = [instance_field(d.applied_field, t_stop, field_schedule) for d in devices]
         # contexts of their own (not the per-device cache): their launch shapes are the batch's
         self.grids = [DeviceGrid(d.params, d.idx, d.material, precision, kmax, "gmres") for d in devices]
         self.x = [g.pack(x0) for g, x0 in zip(self.grids, x0s)]
@@ -86,8 +109,7 @@ class BatchedTrapezoidal:
         jvp = L.TDGL_JVP_ANALYTIC if precision == "mixed" else L.TDGL_JVP_FD
         self.opts = L.TrapOpts(float(t_stop), float(dt), float(dt_min), float(newton_tol_f), float(newton_tol_dx),
                                float(tol_gcr), float(eps_mf), int(newton_max_iter), 0, int(bool(adaptive)), jvp)
-        self.fields = [L.Field(float(d.applied_field.Bx), float(d.applied_field.By), float(d.applied_field.Bz),
-                               1.0, 0.0, float(t_stop), 0, 1) for d in devices]
+        self.fields = fields
         self.totals = {"steps": 0, "newton_iters": 0, "krylov_iters": 0, "rejections": 0}
         self.sms = torch.cuda.get_device_properties(self.grids[0].device).multi_processor_count
         self.shape = (None, -1)                # (nodes per thread or None: single-instance shapes, fused)

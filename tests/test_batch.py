@@ -63,6 +63,24 @@ def test_block_rule():
     assert launch_blocks(10 ** 8, 1, 148) == (8 * 148, 5 * 148)
 
 
+def test_instance_field_constant_and_schedule():
+    """Constant field by default; with field_schedule the AppliedField's
+    schedule against t_stop, as the device evaluates it for ``solve``."""
+    import nanowire_tdgl_b200 as tb
+    from nanowire_tdgl_b200.batch import instance_field
+    af = tb.AppliedField(Bx=0.1, By=-0.2, Bz=0.5, t_on_fraction=0.8, ramp=True, ramp_fraction=0.25)
+    c = instance_field(af, 1e30, False)
+    assert (c.Bx, c.By, c.Bz, c.constant) == (0.1, -0.2, 0.5, 1)
+    s = instance_field(af, 2.0, True)
+    assert (s.Bx, s.By, s.Bz) == (0.1, -0.2, 0.5)
+    assert (s.constant, s.t_field_stop, s.t_on_fraction, s.ramp_fraction, s.ramp) == (0, 2.0, 0.8, 0.25, 1)
+    with pytest.raises(ValueError):
+        instance_field(af, float("inf"), True)
+    with pytest.raises(ValueError):
+        instance_field(tb.AppliedField(field_func=lambda t, ts: (0.0, 0.0, t)), 1.0, True)
+    assert instance_field(tb.AppliedField(field_func=lambda t, ts: (0.0, 0.0, t)), 1.0, False).constant == 1
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("precision", ["mixed", "fp64"])
 @pytest.mark.parametrize("shape", [(None, -1), (2, 0), (2, 1)])
