@@ -108,3 +108,37 @@ def test_fast_path_covers_interior(host_lib):
     slow = (nf & 1).astype(bool).reshape(dev.params.Nz - 1, dev.params.Ny - 1, dev.params.Nx - 1)
     assert not slow[1:-2, 1:-2, 1:-2].any()
     assert slow[0].all() and slow[-2:].all()
+
+
+@pytest.mark.parametrize("periodic", [(False, False, False), (True, True, True), (True, False, True)])
+def test_ghost_link_flags(host_lib, periodic):
+    """NF_GHOSTLF (bit 6) marks exactly the face nodes whose face copy lands
+    on a ghost node that carries hole links (the copy across x = 1 lands on
+    i = 0, or i = Nx when x is periodic; likewise for the other faces), for
+    holes that reach the x, y and z faces."""
+    import nanowire_tdgl_b200 as tb
+    px, py, pz = periodic
+    p = tb.SimulationParameters(Nx=30, Ny=20, Nz=12, hx=0.5, hy=0.5, hz=0.5, kappa=2.0,
+                                periodic_x=px, periodic_y=py, periodic_z=pz)
+    dev = tb.Device(p, applied_field=tb.AppliedField(Bz=0.4, t_on_fraction=1.0))
+    dev.add_hole([(0.0, 3.0), (4.0, 3.0), (4.0, 6.0), (0.0, 6.0)])                              # x = 0 face
+    dev.add_hole([(8.0, 7.0), (12.0, 7.0), (12.0, 10.0), (8.0, 10.0)], z_range=(0, 5))      # y = Ny, z = 0
+    Nx, Ny, Nz = p.Nx, p.Ny, p.Nz
+    hit = np.zeros((Nz + 1) * (Ny + 1) * (Nx + 1), bool)
+    for a in "xyz":
+        hit[np.asarray(getattr(dev.idx, f"hole_{a}_bc_mask"), dtype=np.int64)] = True
+    hit = hit.reshape(Nz + 1, Ny + 1, Nx + 1)
+    want = np.zeros((Nz - 1, Ny - 1, Nx - 1), bool)            # interior nodes, [k-1, j-1, i-1]
+    want[:, :, 0] |= hit[1:Nz, 1:Ny, Nx if px else 0]
+    want[:, :, -1] |= hit[1:Nz, 1:Ny, 0 if px else Nx]
+    want[:, 0, :] |= hit[1:Nz, Ny if py else 0, 1:Nx]
+    want[:, -1, :] |= hit[1:Nz, 0 if py else Ny, 1:Nx]
+    want[0, :, :] |= hit[Nz if pz else 0, 1:Ny, 1:Nx]
+    want[-1, :, :] |= hit[0 if pz else Nz, 1:Ny, 1:Nx]
+    assert want.any()
+    g, md, keep, npad, nc = _setup(host_lib, dev)
+    nf = np.zeros(p.n_interior, dtype=np.uint8)
+    assert host_lib.host_nflags(C.byref(g), C.byref(md), nf.ctypes.data) == 0
+    got = (nf & (1 << 6)).astype(bool).reshape(Nz - 1, Ny - 1, Nx - 1)
+    assert np.array_equal(got, want)
+    assert not got[1:-1, 1:-1, 1:-1].any()
