@@ -705,7 +705,7 @@ def run_batched(a, rank: int = 0, world: int = 1):
             "counters": cnt,
             "max_rel_l2_psi2_batched_vs_looping": max_over_ranks(max(rel), dist, "cuda"),
             "note": "batched and looping differ in launch shapes (reduction partitions) and, when the autotuner "
-                    "picks another degree than the default 5, in the preconditioner (converged states agree to "
+                    "picks another degree than the single-instance default 10, in the preconditioner (converged states agree to "
                     "the Newton tolerance); at equal shapes and degree the results are bit-identical",
             "device_memory_in_use_gb": (total - free) / 1e9,
             "clocks": clk}
