@@ -24,6 +24,7 @@ __all__ = [
 from .solvers import (DeviceRHS, FieldSchedule, eval_f, forward_euler, make_eval_f, newton_gcr_trap, solve,
                       tgcr_matrix_free_trap, trapezoidal)
 from .solution import Solution
+from .hdf5 import load_solution, save_solution
 
 __all__ += ["DeviceRHS", "FieldSchedule", "eval_f", "forward_euler", "make_eval_f", "newton_gcr_trap",
             "solve", "tgcr_matrix_free_trap", "trapezoidal", "Solution"]
@@ -32,7 +33,7 @@ from .adjoint import box_mean_psi2, rhs, trapezoidal_gradient
 __all__ += ["box_mean_psi2", "rhs", "trapezoidal_gradient"]
 from .batch import BatchedTrapezoidal
 
-__all__ += ["BatchedTrapezoidal"]
+__all__ += ["BatchedTrapezoidal", "load_solution", "save_solution"]
 from .analysis import (check_steady_state, compute_convergence_metrics, count_hole_flux_quanta,
                        count_vortices_plaquette, count_vortices_polygon, find_vortex_cores, plaquette_windings)
 

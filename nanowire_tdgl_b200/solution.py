@@ -120,3 +120,16 @@ class Solution:
 
     def psi_squared_2d(self, step: int = -1, slice_z: int = 0):
         return np.abs(self._reshape_interior(self.psi(step), slice_z)) ** 2
+
+    def save(self, filename: str) -> None:
+        """HDF5 file in the layout of src/tdgl3d/core/solution.py:400-461
+        (times, states, parameters, grid indices, metadata; needs h5py)."""
+        from .hdf5 import save_full
+        save_full(self, filename)
+
+    @staticmethod
+    def load(filename: str) -> "Solution":
+        """A ``save`` file (src/tdgl3d/core/solution.py:463-549); the device
+        is not stored, so ``device`` is None."""
+        from .hdf5 import load_full
+        return load_full(filename)
