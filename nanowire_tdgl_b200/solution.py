@@ -121,6 +121,28 @@ class Solution:
     def psi_squared_2d(self, step: int = -1, slice_z: int = 0):
         return np.abs(self._reshape_interior(self.psi(step), slice_z)) ** 2
 
+    def count_vortices(self, device, slice_z: int = 0, step: int = -1, method: str = "plaquette", **kwargs):
+        """Vortices of one slice by ``method`` (src/tdgl3d/core/solution.py:302-354):
+        "plaquette" (``count_vortices_plaquette``: count, positions, windings),
+        "polygon" (``count_vortices_polygon``, needs ``polygon_points``) or
+        "cores" (``find_vortex_cores``); ValueError for anything else."""
+        from . import analysis
+        if method == "plaquette":
+            return analysis.count_vortices_plaquette(self, device, slice_z, step, **kwargs)
+        if method == "polygon":
+            if "polygon_points" not in kwargs:
+                raise ValueError("polygon method requires polygon_points argument")
+            return analysis.count_vortices_polygon(self, device, kwargs["polygon_points"], slice_z, step)
+        if method == "cores":
+            return analysis.find_vortex_cores(self, device, slice_z, step, **kwargs)
+        raise ValueError(f"Unknown method: {method}")
+
+    def check_steady_state(self, device=None, window_size: int = 10, psi_threshold: float = 1e-4,
+                           current_threshold: float = 1e-4, start_step: int = 20):
+        """``check_steady_state`` on this solution (src/tdgl3d/core/solution.py:356-396)."""
+        from . import analysis
+        return analysis.check_steady_state(self, device, window_size, psi_threshold, current_threshold, start_step)
+
     def save(self, filename: str) -> None:
         """HDF5 file in the layout of src/tdgl3d/core/solution.py:400-461
         (times, states, parameters, grid indices, metadata; needs h5py)."""

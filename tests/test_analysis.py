@@ -83,6 +83,32 @@ def test_host_polygon_and_cores_against_golden():
         assert np.array_equal(cores.reshape(-1, 2), G[f"v3_{k}_cores"])
 
 
+def test_solution_methods_dispatch_like_the_reference(monkeypatch):
+    """Solution.count_vortices / check_steady_state (solution.py:302-396):
+    the host methods give the golden answers, the device ones are forwarded
+    with the caller's arguments, bad methods raise ValueError."""
+    from nanowire_tdgl_b200 import analysis
+    d = _dev3()
+    x = G["v3_x"]
+    sol = _sol(d, [0.0, 1.0], np.stack([x * 0.5, x], axis=1))
+    poly = np.array([[2, 2], [16, 2], [16, 18], [2, 18]])
+    got = sol.count_vortices(d, slice_z=1, method="polygon", polygon_points=poly)
+    assert abs(got - float(G["v3_1_poly"])) < 1e-12
+    cores = sol.count_vortices(d, slice_z=1, method="cores", threshold=0.1, separation=2)
+    assert np.array_equal(cores.reshape(-1, 2), G["v3_1_cores"])
+    calls = []
+    monkeypatch.setattr(analysis, "count_vortices_plaquette", lambda *a, **k: calls.append(("plaq", a, k)) or 7)
+    monkeypatch.setattr(analysis, "check_steady_state", lambda *a, **k: calls.append(("steady", a, k)) or 8)
+    assert sol.count_vortices(d, 2, 0, winding_threshold=0.5) == 7
+    assert sol.check_steady_state(d, 5, 1e-3, 1e-2, 3) == 8
+    assert calls == [("plaq", (sol, d, 2, 0), {"winding_threshold": 0.5}),
+                     ("steady", (sol, d, 5, 1e-3, 1e-2, 3), {})]
+    with pytest.raises(ValueError):
+        sol.count_vortices(d, method="polygon")
+    with pytest.raises(ValueError):
+        sol.count_vortices(d, method="other")
+
+
 @pytest.mark.gpu
 def test_device_plaquette_windings_match_oracle():
     import nanowire_tdgl_b200 as tb
